@@ -1,0 +1,173 @@
+/*
+ * sgnb.h -- C ABI of the B200 (sm_100a) implementation of the 2D hyperbolic-SGN
+ * flux-reconstruction right-hand side and its adaptive Bogacki-Shampine 3(2) loop.
+ *
+ * Plain C: pointers, sizes and status codes only. Every entry point names the
+ * interface of the reference project (gsalanglada/sgn-hyperbolic-gpu) that it
+ * replaces. A header-only C++ wrapper with the reference's member signatures is in
+ * sgnb.hpp.
+ *
+ * State layout (unchanged from the reference, src/solver/sgn2d.h:22-27):
+ * variable-major doubles U[v * Nd + e * 25 + a + 5 b], v in (h, hu, hv, hw, hp),
+ * element e = ex + Nx ey, node (a, b) of the 5 x 5 GLL grid, Nd = 25 Nx Ny.
+ *
+ * Errors: every function returns an sgnb_status; nothing aborts the process
+ * (the reference aborts on CUDA errors, src/cuda/sgn2d_cuda.cu:29-37).
+ * sgnb_last_error() gives a message for the last failure on a context.
+ * Threading: a context belongs to one host thread at a time; its work runs on its
+ * own CUDA stream on the device chosen at creation.
+ */
+#ifndef SGNB_H
+#define SGNB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SGNB_OK = 0,
+  SGNB_ERR_INVALID = 1,      /* bad argument or size (reference: std::invalid_argument) */
+  SGNB_ERR_UNSUPPORTED = 2,  /* valid for the reference, not built here (P != 4, ...) */
+  SGNB_ERR_CUDA = 3,         /* CUDA runtime error; the message names the call */
+  SGNB_ERR_NAN = 4,          /* non-finite embedded error: the run stopped */
+  SGNB_ERR_DTMIN = 5,        /* step size fell below dtMin (reference stats.aborted) */
+  SGNB_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
+  SGNB_ERR_NOMEM = 7,        /* device allocation failed */
+  SGNB_ERR_NO_DEVICE = 8     /* no CUDA device visible */
+} sgnb_status;
+
+enum { SGNB_BC_PERIODIC = 0, SGNB_BC_WALL = 1 };
+
+/* Arithmetic modes of the FP64 path. */
+enum {
+  SGNB_FP64_EXACT = 0, /* reference operation order, no FMA: bit-identical to the CPU */
+  SGNB_FP64_FAST = 1   /* FMA + reciprocals: within 1e-13 relative per field */
+};
+
+/* Built-in still-depth profiles H(x, y); SGNB_BATHY_ARRAYS takes precomputed arrays.
+ * Parameter vectors are documented in sgnb_setup.cpp. */
+enum {
+  SGNB_BATHY_NONE = 0,      /* H = 0 (the reference's empty stillDepth, sgn2d.h:55) */
+  SGNB_BATHY_CONST = 1,     /* p0 */
+  SGNB_BATHY_GAUSS = 2,     /* p0 - p1 exp(-((x-p2)^2 + (y-p3)^2) / p4) */
+  SGNB_BATHY_SHOAL = 3,     /* elliptic shoal on a plane */
+  SGNB_BATHY_GAUSS_SUM = 4, /* plane minus a sum of Gaussian bumps */
+  SGNB_BATHY_CELLS = 5,     /* bilinear interpolant of a grid of cell means */
+  SGNB_BATHY_ARRAYS = 100   /* Hnod .. HfaceYEnd given by the caller */
+};
+
+/* Construction parameters; mirrors the arguments of
+ * SGN2D(int P, int Nx, int Ny, double Lx, double Ly, const sgn2d::Params&,
+ *       std::function<double(double,double)> stillDepth, PointSet)
+ * (src/solver/sgn2d.h:57-59) plus the sgn2d::Params fields (src/physics/sgn_flux2d.h:57-62).
+ * Call sgnb_desc_init() first. */
+typedef struct {
+  int P, Nx, Ny;             /* only P = 4 is built; Nx, Ny >= 2 */
+  double Lx, Ly;
+  double g, c, gamma, nManning; /* nManning must be 0 (Manning friction is not built) */
+  int bc_x, bc_y;            /* SGNB_BC_*; walls are an addition to the reference */
+  int precision;             /* SGNB_FP64_* */
+  int device;                /* CUDA device ordinal */
+  /* FR tables of FROperators1D (src/core/fr_operators.h:68-89); all NULL = built here */
+  const double *nodes, *D, *lL, *lR, *gLp, *gRp, *qw;
+  int bathy_kind;            /* SGNB_BATHY_* */
+  const double* bathy_par;
+  int n_bathy_par;
+  /* SGNB_BATHY_ARRAYS: the SGN2D accessors stillDepthNodal/GradX/GradY/FaceX/FaceY
+   * (sgn2d.h:94-98; Nd, Nd, Nd, 5 Nx Ny, 5 Nx Ny doubles) and, for walls, the depth on
+   * the right edge (5 Ny, sampled at x = Nx hx) and top edge (5 Nx, at y = Ny hy). */
+  const double *Hnod, *Hx, *Hy, *HfaceX, *HfaceY, *HfaceXEnd, *HfaceYEnd;
+} sgnb_desc;
+
+/* AdaptiveRKOptions (src/solver/rk.h:53-61). */
+typedef struct {
+  double atol, rtol, dtMin, dtMax, safety, facMin, facMax;
+} sgnb_rk_opts;
+
+/* AdaptiveRKStats (src/solver/rk.h:64-72) plus the attempt count and a status. */
+typedef struct {
+  long long accepted, rejected, rhsEvals, attempts;
+  double tReached, dtLast, maxNormLast;
+  int aborted;   /* 1: dt < dtMin (as the reference); 2: non-finite error */
+  int status;    /* sgnb_status of the run */
+} sgnb_rk_stats;
+
+typedef struct sgnb_ctx sgnb_ctx;
+
+/* Defaults: P 4, Nx = Ny = 2, Lx = Ly = 1, Params{g 9.81, c 0, gamma 1.5, n 0},
+ * periodic, FP64 exact, device 0, tables built here, H = 0. */
+void sgnb_desc_init(sgnb_desc* d);
+/* Defaults of AdaptiveRKOptions (src/solver/rk.h:53-61). */
+void sgnb_rk_opts_init(sgnb_rk_opts* o);
+
+/* Replaces SGN2DCuda::SGN2DCuda(const SGN2D&) (src/cuda/sgn2d_cuda.h:33): allocates the
+ * device state and uploads tables and bathymetry. */
+int sgnb_create(const sgnb_desc* d, sgnb_ctx** out);
+/* Replaces SGN2DCuda::~SGN2DCuda (src/cuda/sgn2d_cuda.h:34). NULL is allowed. */
+int sgnb_destroy(sgnb_ctx* ctx);
+
+/* SGN2D::nDof (src/solver/sgn2d.h:64): nodes per field. State size is 5 * this. */
+long long sgnb_ndof(const sgnb_ctx* ctx);
+
+/* SGN2DCuda::upload / download (src/cuda/sgn2d_cuda.h:41-42): host <-> device state. */
+int sgnb_upload(sgnb_ctx* ctx, const double* U_host);
+int sgnb_download(sgnb_ctx* ctx, double* U_host);
+
+/* SGN2DCuda::rhsOnce (src/cuda/sgn2d_cuda.h:43): dU = R(uploaded state), to the host. */
+int sgnb_rhs_once(sgnb_ctx* ctx, double* dU_host);
+/* SGN2D::rhs (src/solver/sgn2d.h:78): dU = R(U) for host arrays; the uploaded state is
+ * left untouched. */
+int sgnb_rhs_host(sgnb_ctx* ctx, const double* U_host, double* dU_host);
+/* SGN2DCuda::rhsDevice (src/cuda/sgn2d_cuda.h:51), public here: dU = R(U) for device
+ * arrays on a caller stream (cudaStream_t, NULL = the context stream). Asynchronous. */
+int sgnb_rhs_device(sgnb_ctx* ctx, const double* U_dev, double* dU_dev, void* stream);
+
+/* SGN2DCuda::integrateAdaptive (src/cuda/sgn2d_cuda.h:46-47), the device-resident form
+ * of integrateAdaptive (src/solver/rk.h:78-80): integrates the uploaded state in place.
+ * opts NULL = defaults. Returns SGNB_OK also when stats->aborted is set (as the
+ * reference returns normally with stats.aborted). */
+int sgnb_integrate_adaptive(sgnb_ctx* ctx, double t0, double tEnd, double dt0,
+                            const sgnb_rk_opts* opts, sgnb_rk_stats* stats);
+/* n consecutive bs3Step (src/solver/rk.h:50) steps of the uploaded state with the
+ * given step sizes, starting at t0: the frozen-dt replay of an accepted sequence. */
+int sgnb_bs3_steps(sgnb_ctx* ctx, double t0, const double* dts, long long n);
+
+/* Attempt log of the last sgnb_integrate_adaptive / sgnb_bs3_steps call: per attempt
+ * (t, dt, errNorm, accepted as 1.0 / 0.0), up to 65536 attempts. Copies min(cap, n)
+ * rows into out and sets *n to the number recorded. No reference counterpart (the
+ * reference keeps only AdaptiveRKStats); it exposes the controller's dt sequence. */
+int sgnb_attempt_log(sgnb_ctx* ctx, double* out, long long cap, long long* n);
+
+/* SGN2D::maxWaveSpeed / cflTimeStep / mass / energy (src/solver/sgn2d.h:85-90) of the
+ * uploaded state, reduced on the device. */
+int sgnb_max_wave_speed(sgnb_ctx* ctx, double* out);
+int sgnb_cfl_time_step(sgnb_ctx* ctx, double cfl, double* out);
+int sgnb_mass(sgnb_ctx* ctx, double* out);
+int sgnb_energy(sgnb_ctx* ctx, double* out);
+
+/* Host-side set-up queries (no device work). */
+/* SGN2D::nodeCoords (src/solver/sgn2d.h:70). */
+int sgnb_node_coords(const sgnb_ctx* ctx, double* x, double* y);
+/* Device pointers of the state buffer that holds u and of the context stream, for
+ * callers that manage device memory themselves. */
+int sgnb_state_device_ptr(sgnb_ctx* ctx, double** U_dev, void** stream);
+
+/* FROperators1D tables for degree P (src/core/fr_operators.cpp:134-200), computed on
+ * the host without a device. Sizes P+1, (P+1)^2 for D. */
+int sgnb_fr_tables(int P, double* nodes, double* D, double* lL, double* lR, double* gLp,
+                   double* gRp, double* qw);
+/* The bathymetry arrays sgnb_create would upload for d (SGN2D ctor,
+ * src/solver/sgn2d.cpp:30-84), on the host without a device. Any pointer may be NULL. */
+int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* Hy,
+                          double* HfaceX, double* HfaceY, double* HfaceXEnd,
+                          double* HfaceYEnd);
+
+const char* sgnb_status_string(int status);
+/* Message of the last failure on ctx (or of the last failed sgnb_create when NULL). */
+const char* sgnb_last_error(const sgnb_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGNB_H */

@@ -1,0 +1,591 @@
+// sgnb_api.cu -- implementation of the C ABI declared in include/sgnb.h.
+//
+// The context owns the device state of one solver: the bathymetry statics, the state
+// ping-pong pair U[2], the FSAL pair K1[2] (k1 / k4), the stage derivatives K2, K3,
+// the per-CTA error partials and the device-resident controller state. An adaptive
+// integration is a sequence of graph launches, each replaying a chunk of attempts
+// (stage 2, stage 3, end-point stage, controller); the host reads the controller back
+// once per chunk instead of once per step (the reference copies error partials to the
+// host every step, src/cuda/sgn2d_cuda.cu:506-516).
+#include "sgnb.h"
+#include "sgnb_device.h"
+#include "sgnb_setup.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace sgnb;
+
+struct sgnb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  sgnb_desc desc{};
+  int precision = SGNB_FP64_EXACT;
+  Mesh mesh;
+  FrTables tab;
+  long long Nd = 0, ntot = 0;
+  RhsConsts C{};
+  double* Hbuf = nullptr;  // one allocation holding all statics
+  double* U[2] = {nullptr, nullptr};
+  double* K1[2] = {nullptr, nullptr};
+  double* K2 = nullptr;
+  double* K3 = nullptr;
+  double* partials = nullptr;
+  int nblk = 0;
+  double* diag = nullptr;  // diagnostic partials
+  int ndiag = 0;
+  CtrlState* dctrl = nullptr;
+  CtrlState* hctrl = nullptr;  // pinned mirror
+  double* dtList = nullptr;
+  long long dtCap = 0;
+  double* alog = nullptr;  // device attempt log of the last integration
+  static constexpr long long kLogCap = 1 << 16;
+  cudaGraphExec_t chunk = nullptr;
+  int chunkLen = 0;
+  cudaEvent_t evRead = nullptr;
+  int cur = 0;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(sgnb_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg; else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(sgnb_ctx* c, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return fail(c, e == cudaErrorMemoryAllocation ? SGNB_ERR_NOMEM : SGNB_ERR_CUDA, m);
+}
+
+#define SGNB_CU(ctx, call)                          \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+cudaError_t launch(sgnb_ctx* c, int mode, const StageArgs& A, cudaStream_t s) {
+  return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(mode, c->C, A, s)
+                                        : dev::launch_fused_exact(mode, c->C, A, s);
+}
+
+StageArgs base_args(sgnb_ctx* c) {
+  StageArgs A{};
+  A.U[0] = c->U[0]; A.U[1] = c->U[1];
+  A.K1[0] = c->K1[0]; A.K1[1] = c->K1[1];
+  A.K2 = c->K2; A.K3 = c->K3;
+  A.ctrl = c->dctrl;
+  A.partials = c->partials;
+  return A;
+}
+
+int set_device(sgnb_ctx* c) {
+  SGNB_CU(c, cudaSetDevice(c->device));
+  return SGNB_OK;
+}
+
+int check_desc(const sgnb_desc* d) {
+  if (!d) return fail(nullptr, SGNB_ERR_INVALID, "desc is NULL");
+  if (d->Nx < 2 || d->Ny < 2) return fail(nullptr, SGNB_ERR_INVALID, "SGN2D: Nx,Ny >= 2");
+  if (d->P != 4) return fail(nullptr, SGNB_ERR_UNSUPPORTED, "only P = 4 is built");
+  if (!(d->Lx > 0) || !(d->Ly > 0)) return fail(nullptr, SGNB_ERR_INVALID, "Lx, Ly must be > 0");
+  if (d->nManning != 0.0)
+    return fail(nullptr, SGNB_ERR_UNSUPPORTED, "Manning friction is not built");
+  if (d->bc_x < 0 || d->bc_x > 1 || d->bc_y < 0 || d->bc_y > 1)
+    return fail(nullptr, SGNB_ERR_INVALID, "bc must be SGNB_BC_PERIODIC or SGNB_BC_WALL");
+  if (d->precision != SGNB_FP64_EXACT && d->precision != SGNB_FP64_FAST)
+    return fail(nullptr, SGNB_ERR_UNSUPPORTED, "unknown precision mode");
+  if ((long long)d->Nx * d->Ny > (1ll << 31) / 25)
+    return fail(nullptr, SGNB_ERR_INVALID, "mesh too large");
+  if (d->bathy_kind == SGNB_BATHY_ARRAYS) {
+    if (!d->Hnod || !d->Hx || !d->Hy || !d->HfaceX || !d->HfaceY)
+      return fail(nullptr, SGNB_ERR_INVALID, "SGNB_BATHY_ARRAYS needs Hnod, Hx, Hy, HfaceX, HfaceY");
+    if ((d->bc_x == SGNB_BC_WALL && !d->HfaceXEnd) || (d->bc_y == SGNB_BC_WALL && !d->HfaceYEnd))
+      return fail(nullptr, SGNB_ERR_INVALID, "walls need HfaceXEnd / HfaceYEnd");
+  } else {
+    const int need = bathy_param_count(d->bathy_kind, d->bathy_par, d->n_bathy_par);
+    if (need < 0) return fail(nullptr, SGNB_ERR_INVALID, "unknown bathy_kind");
+    if (need > 0 && (!d->bathy_par || d->n_bathy_par < need))
+      return fail(nullptr, SGNB_ERR_INVALID, "bathy_par too short for bathy_kind");
+  }
+  return SGNB_OK;
+}
+
+// FR tables: the caller's (copied from a reference FROperators1D) or built here.
+int tables_for(const sgnb_desc* d, FrTables& t) {
+  fr_tables(d->P, t);
+  const int n = d->P + 1;
+  if (d->nodes) std::memcpy(t.nodes, d->nodes, n * sizeof(double));
+  if (d->D) std::memcpy(t.D, d->D, n * n * sizeof(double));
+  if (d->lL) std::memcpy(t.lL, d->lL, n * sizeof(double));
+  if (d->lR) std::memcpy(t.lR, d->lR, n * sizeof(double));
+  if (d->gLp) std::memcpy(t.gLp, d->gLp, n * sizeof(double));
+  if (d->gRp) std::memcpy(t.gRp, d->gRp, n * sizeof(double));
+  if (d->qw) std::memcpy(t.qw, d->qw, n * sizeof(double));
+  // the kernels read face traces as the edge nodes: require GLL unit rows
+  for (int j = 0; j < n; ++j) {
+    if (t.lL[j] != (j == 0 ? 1.0 : 0.0) || t.lR[j] != (j == n - 1 ? 1.0 : 0.0))
+      return fail(nullptr, SGNB_ERR_UNSUPPORTED, "only Gauss-Lobatto points are built");
+  }
+  return SGNB_OK;
+}
+
+Mesh mesh_for(const sgnb_desc* d) {
+  Mesh m;
+  m.Nx = d->Nx; m.Ny = d->Ny; m.Lx = d->Lx; m.Ly = d->Ly;
+  m.hx = d->Lx / d->Nx; m.hy = d->Ly / d->Ny;  // mesh2d.h:27-28
+  return m;
+}
+
+void fill_consts(sgnb_ctx* c) {
+  RhsConsts& C = c->C;
+  const sgnb_desc& d = c->desc;
+  C.Nx = d.Nx; C.Ny = d.Ny;
+  C.bcx = d.bc_x; C.bcy = d.bc_y;
+  C.Nd = c->Nd;
+  C.g = d.g;
+  C.halfg = 0.5 * d.g;
+  C.gamma = d.gamma;
+  C.c2 = d.c * d.c;
+  C.mc2 = -d.c * d.c;
+  C.m2c2 = -2.0 * C.c2;
+  C.Jx = 0.5 * c->mesh.hx;  // mesh2d.h:49-50
+  C.Jy = 0.5 * c->mesh.hy;
+  C.iJx = 1.0 / C.Jx;
+  C.iJy = 1.0 / C.Jy;
+  for (int k = 0; k < 25; ++k) C.D[k] = c->tab.D[k];
+  for (int k = 0; k < 5; ++k) {
+    C.gLp[k] = c->tab.gLp[k];
+    C.gRp[k] = c->tab.gRp[k];
+  }
+}
+
+int build_chunk_graph(sgnb_ctx* c, int len) {
+  if (c->chunk && c->chunkLen == len) return SGNB_OK;
+  if (c->chunk) {
+    cudaGraphExecDestroy(c->chunk);
+    c->chunk = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  SGNB_CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < len && e == cudaSuccess; ++k) {
+    StageArgs A = base_args(c);
+    A.kin_k2 = 0; A.coef = 0.5; A.out = c->K2;  // k2 = R(u + dt/2 k1)
+    e = launch(c, 1, A, c->stream);
+    if (e != cudaSuccess) break;
+    A.kin_k2 = 1; A.coef = 0.75; A.out = c->K3;  // k3 = R(u + 3dt/4 k2)
+    e = launch(c, 1, A, c->stream);
+    if (e != cudaSuccess) break;
+    StageArgs F = base_args(c);
+    e = launch(c, 2, F, c->stream);  // uNew, k4 = R(uNew), error partials
+    if (e != cudaSuccess) break;
+    e = dev::launch_controller(c->dctrl, c->partials, c->nblk, c->ntot, c->stream);
+  }
+  cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "capture of the attempt chunk"); }
+  if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&c->chunk, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+  c->chunkLen = len;
+  return SGNB_OK;
+}
+
+// Drive the device-resident loop until the controller reports done.
+int run_loop(sgnb_ctx* c) {
+  int rc = build_chunk_graph(c, 16);
+  if (rc) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
+  // FSAL head: k1 = R(u)
+  {
+    StageArgs A = base_args(c);
+    A.in = c->U[c->cur];
+    A.out = c->K1[c->cur];
+    SGNB_CU(c, launch(c, 0, A, c->stream));
+  }
+  // two chunks in flight: enqueue chunk k+1 before waiting for chunk k's readback
+  SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
+  SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaEventRecord(c->evRead, c->stream));
+  for (long long guard = 0;; ++guard) {
+    SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
+    SGNB_CU(c, cudaEventSynchronize(c->evRead));
+    if (c->hctrl->done) break;
+    SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
+    SGNB_CU(c, cudaEventRecord(c->evRead, c->stream));
+  }
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  SGNB_CU(c, cudaMemcpy(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost));
+  c->cur = c->hctrl->cur;
+  return SGNB_OK;
+}
+
+void init_ctrl(sgnb_ctx* c, CtrlState& s, const sgnb_rk_opts& o) {
+  std::memset(&s, 0, sizeof(s));
+  s.log = c->alog;
+  s.logCap = sgnb_ctx::kLogCap;
+  s.atol = o.atol; s.rtol = o.rtol; s.dtMin = o.dtMin; s.dtMax = o.dtMax;
+  s.safety = o.safety; s.facMin = o.facMin; s.facMax = o.facMax;
+  const int orderLow = 2;                          // rk.cpp:71-76
+  const double expo = 1.0 / (orderLow + 1.0);
+  s.alpha = 0.7 * expo;
+  s.beta = 0.4 * expo;
+}
+
+}  // namespace
+
+extern "C" {
+
+void sgnb_desc_init(sgnb_desc* d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof(*d));
+  d->P = 4; d->Nx = 2; d->Ny = 2; d->Lx = 1.0; d->Ly = 1.0;
+  d->g = 9.81; d->c = 0.0; d->gamma = 1.5; d->nManning = 0.0;
+  d->bc_x = SGNB_BC_PERIODIC; d->bc_y = SGNB_BC_PERIODIC;
+  d->precision = SGNB_FP64_EXACT;
+  d->bathy_kind = SGNB_BATHY_NONE;
+}
+
+void sgnb_rk_opts_init(sgnb_rk_opts* o) {
+  if (!o) return;
+  o->atol = 1e-8; o->rtol = 1e-6; o->dtMin = 1e-13; o->dtMax = 1e30;
+  o->safety = 0.9; o->facMin = 0.2; o->facMax = 5.0;
+}
+
+int sgnb_fr_tables(int P, double* nodes, double* D, double* lL, double* lR, double* gLp,
+                   double* gRp, double* qw) {
+  FrTables t;
+  if (!fr_tables(P, t)) return fail(nullptr, SGNB_ERR_UNSUPPORTED, "P out of range");
+  const int n = P + 1;
+  if (nodes) std::memcpy(nodes, t.nodes, n * sizeof(double));
+  if (D) std::memcpy(D, t.D, n * n * sizeof(double));
+  if (lL) std::memcpy(lL, t.lL, n * sizeof(double));
+  if (lR) std::memcpy(lR, t.lR, n * sizeof(double));
+  if (gLp) std::memcpy(gLp, t.gLp, n * sizeof(double));
+  if (gRp) std::memcpy(gRp, t.gRp, n * sizeof(double));
+  if (qw) std::memcpy(qw, t.qw, n * sizeof(double));
+  return SGNB_OK;
+}
+
+int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* Hy,
+                          double* HfaceX, double* HfaceY, double* HfaceXEnd,
+                          double* HfaceYEnd) {
+  int rc = check_desc(d);
+  if (rc) return rc;
+  if (d->bathy_kind == SGNB_BATHY_ARRAYS) return fail(nullptr, SGNB_ERR_INVALID, "arrays given");
+  FrTables t;
+  if ((rc = tables_for(d, t))) return rc;
+  const Mesh m = mesh_for(d);
+  Bathymetry b;
+  bathymetry(m, t, d->bathy_kind, d->bathy_par, b);
+  auto cp = [](const std::vector<double>& v, double* o) {
+    if (o) std::memcpy(o, v.data(), v.size() * sizeof(double));
+  };
+  cp(b.Hnod, Hnod); cp(b.Hx, Hx); cp(b.Hy, Hy); cp(b.HfX, HfaceX); cp(b.HfY, HfaceY);
+  cp(b.HfXEnd, HfaceXEnd); cp(b.HfYEnd, HfaceYEnd);
+  return SGNB_OK;
+}
+
+int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
+  if (!out) return fail(nullptr, SGNB_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int rc = check_desc(d);
+  if (rc) return rc;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, SGNB_ERR_NO_DEVICE, "no CUDA device visible");
+  if (d->device < 0 || d->device >= ndev) return fail(nullptr, SGNB_ERR_INVALID, "bad device ordinal");
+
+  sgnb_ctx* c = new sgnb_ctx();
+  c->desc = *d;
+  c->desc.nodes = c->desc.D = c->desc.lL = c->desc.lR = nullptr;
+  c->desc.gLp = c->desc.gRp = c->desc.qw = nullptr;
+  c->desc.bathy_par = nullptr;
+  c->desc.Hnod = c->desc.Hx = c->desc.Hy = c->desc.HfaceX = c->desc.HfaceY = nullptr;
+  c->desc.HfaceXEnd = c->desc.HfaceYEnd = nullptr;
+  c->device = d->device;
+  c->precision = d->precision;
+  if ((rc = tables_for(d, c->tab))) { delete c; return rc; }
+  c->mesh = mesh_for(d);
+  const long long ne = (long long)d->Nx * d->Ny;
+  c->Nd = ne * 25;
+  c->ntot = 5 * c->Nd;
+  auto bail = [&](int code) { sgnb_destroy(c); return code; };
+  if ((rc = set_device(c))) { g_create_error = c->err; delete c; return rc; }
+  e = dev::prepare_fused_exact();
+  if (e == cudaSuccess) e = dev::prepare_fused_fast();
+  if (e != cudaSuccess) { cuda_fail(c, e, "kernel attributes"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
+
+  // statics: Hnod, Hx, Hy (Nd each), HfX, HfY (5 ne each), HfXEnd (5 Ny), HfYEnd (5 Nx)
+  Bathymetry b;
+  if (d->bathy_kind == SGNB_BATHY_ARRAYS) {
+    b.Hnod.assign(d->Hnod, d->Hnod + c->Nd);
+    b.Hx.assign(d->Hx, d->Hx + c->Nd);
+    b.Hy.assign(d->Hy, d->Hy + c->Nd);
+    b.HfX.assign(d->HfaceX, d->HfaceX + 5 * ne);
+    b.HfY.assign(d->HfaceY, d->HfaceY + 5 * ne);
+    b.HfXEnd.assign(5 * (size_t)d->Ny, 0.0);
+    b.HfYEnd.assign(5 * (size_t)d->Nx, 0.0);
+    if (d->HfaceXEnd) b.HfXEnd.assign(d->HfaceXEnd, d->HfaceXEnd + 5 * d->Ny);
+    if (d->HfaceYEnd) b.HfYEnd.assign(d->HfaceYEnd, d->HfaceYEnd + 5 * d->Nx);
+  } else {
+    bathymetry(c->mesh, c->tab, d->bathy_kind, d->bathy_par, b);
+  }
+  const size_t nstat = 3 * (size_t)c->Nd + 10 * (size_t)ne + 5 * (size_t)(d->Nx + d->Ny);
+  e = cudaMalloc(&c->Hbuf, nstat * sizeof(double));
+  if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(statics)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
+  double* p = c->Hbuf;
+  auto put = [&](const std::vector<double>& v, const double*& dst) {
+    dst = p;
+    cudaError_t e2 = cudaMemcpy(p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice);
+    p += v.size();
+    return e2;
+  };
+  e = put(b.Hnod, c->C.Hnod);
+  if (e == cudaSuccess) e = put(b.Hx, c->C.Hx);
+  if (e == cudaSuccess) e = put(b.Hy, c->C.Hy);
+  if (e == cudaSuccess) e = put(b.HfX, c->C.HfX);
+  if (e == cudaSuccess) e = put(b.HfY, c->C.HfY);
+  if (e == cudaSuccess) e = put(b.HfXEnd, c->C.HfXEnd);
+  if (e == cudaSuccess) e = put(b.HfYEnd, c->C.HfYEnd);
+  if (e != cudaSuccess) { cuda_fail(c, e, "upload of statics"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
+  fill_consts(c);
+
+  const size_t sbytes = (size_t)c->ntot * sizeof(double);
+  double** bufs[6] = {&c->U[0], &c->U[1], &c->K1[0], &c->K1[1], &c->K2, &c->K3};
+  for (auto* bp : bufs) {
+    e = cudaMalloc(bp, sbytes);
+    if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(state)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
+  }
+  e = cudaMemset(c->U[0], 0, sbytes);
+  c->nblk = dev::fused_grid_blocks(d->Nx, d->Ny);
+  c->ndiag = 592;
+  if (e == cudaSuccess) e = cudaMalloc(&c->partials, 3 * (size_t)c->nblk * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->diag, (size_t)c->ndiag * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->dctrl, sizeof(CtrlState));
+  if (e == cudaSuccess) e = cudaMalloc(&c->alog, 4 * sgnb_ctx::kLogCap * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->hctrl, sizeof(CtrlState));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->evRead, cudaEventDisableTiming);
+  if (e != cudaSuccess) { cuda_fail(c, e, "context buffers"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
+  sgnb_rk_opts o;
+  sgnb_rk_opts_init(&o);
+  init_ctrl(c, *c->hctrl, o);
+  *out = c;
+  return SGNB_OK;
+}
+
+int sgnb_destroy(sgnb_ctx* c) {
+  if (!c) return SGNB_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->chunk) cudaGraphExecDestroy(c->chunk);
+  if (c->evRead) cudaEventDestroy(c->evRead);
+  cudaFree(c->Hbuf);
+  for (int k = 0; k < 2; ++k) { cudaFree(c->U[k]); cudaFree(c->K1[k]); }
+  cudaFree(c->K2); cudaFree(c->K3);
+  cudaFree(c->partials); cudaFree(c->diag); cudaFree(c->dctrl); cudaFree(c->dtList);
+  cudaFree(c->alog);
+  if (c->hctrl) cudaFreeHost(c->hctrl);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return SGNB_OK;
+}
+
+long long sgnb_ndof(const sgnb_ctx* c) { return c ? c->Nd : 0; }
+
+int sgnb_upload(sgnb_ctx* c, const double* U) {
+  if (!c || !U) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(c->U[c->cur], U, c->ntot * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  return SGNB_OK;
+}
+
+int sgnb_download(sgnb_ctx* c, double* U) {
+  if (!c || !U) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(U, c->U[c->cur], c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  return SGNB_OK;
+}
+
+int sgnb_rhs_device(sgnb_ctx* c, const double* Ud, double* dUd, void* stream) {
+  if (!c || !Ud || !dUd) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (Ud == dUd) return fail(c, SGNB_ERR_INVALID, "input and output must not alias");
+  StageArgs A = base_args(c);
+  A.in = Ud;
+  A.out = dUd;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  SGNB_CU(c, launch(c, 0, A, s));
+  return SGNB_OK;
+}
+
+int sgnb_rhs_once(sgnb_ctx* c, double* dU) {
+  if (!c || !dU) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  if (int rc = sgnb_rhs_device(c, c->U[c->cur], c->K2, c->stream)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(dU, c->K2, c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  return SGNB_OK;
+}
+
+int sgnb_rhs_host(sgnb_ctx* c, const double* U, double* dU) {
+  if (!c || !U || !dU) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(c->K3, U, c->ntot * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (int rc = sgnb_rhs_device(c, c->K3, c->K2, c->stream)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(dU, c->K2, c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  return SGNB_OK;
+}
+
+int sgnb_integrate_adaptive(sgnb_ctx* c, double t0, double tEnd, double dt0,
+                            const sgnb_rk_opts* opts, sgnb_rk_stats* st) {
+  if (!c) return fail(c, SGNB_ERR_INVALID, "NULL context");
+  if (int rc = set_device(c)) return rc;
+  sgnb_rk_opts o;
+  if (opts) o = *opts; else sgnb_rk_opts_init(&o);
+  CtrlState& h = *c->hctrl;
+  init_ctrl(c, h, o);
+  h.t = t0;
+  h.tEnd = tEnd;
+  h.dt = (o.dtMax < dt0) ? o.dtMax : dt0;  // std::min(dt0, dtMax), rk.cpp:87
+  h.errPrev = 1.0;
+  h.tReached = t0;
+  h.cur = c->cur;
+  h.rhsEvals = 1;  // FSAL head
+  // loop test and end-time clip of the first attempt (rk.cpp:95-97)
+  if (!(h.t < tEnd - 1e-15 * ((1.0 < std::fabs(tEnd)) ? std::fabs(tEnd) : 1.0))) h.done = 1;
+  else if (h.t + h.dt > tEnd) h.dt = tEnd - h.t;
+  if (c->ntot == 0) h.done = 1;
+  if (int rc = run_loop(c)) return rc;
+  if (st) {
+    st->accepted = h.accepted; st->rejected = h.rejected; st->rhsEvals = h.rhsEvals;
+    st->attempts = h.attempts; st->tReached = h.tReached; st->dtLast = h.dtLast;
+    st->maxNormLast = h.maxNormLast;
+    st->aborted = h.done == 2 ? 1 : (h.done == 3 ? 2 : 0);
+    st->status = h.done == 3 ? SGNB_ERR_NAN : SGNB_OK;
+  }
+  if (h.done == 3) return fail(c, SGNB_ERR_NAN, "non-finite embedded error estimate");
+  return SGNB_OK;
+}
+
+int sgnb_bs3_steps(sgnb_ctx* c, double t0, const double* dts, long long n) {
+  if (!c || (n > 0 && !dts) || n < 0) return fail(c, SGNB_ERR_INVALID, "bad arguments");
+  if (n == 0) return SGNB_OK;
+  if (int rc = set_device(c)) return rc;
+  if (n > c->dtCap) {
+    cudaFree(c->dtList);
+    c->dtList = nullptr;
+    SGNB_CU(c, cudaMalloc(&c->dtList, n * sizeof(double)));
+    c->dtCap = n;
+  }
+  SGNB_CU(c, cudaMemcpy(c->dtList, dts, n * sizeof(double), cudaMemcpyHostToDevice));
+  CtrlState& h = *c->hctrl;
+  sgnb_rk_opts o;
+  sgnb_rk_opts_init(&o);
+  init_ctrl(c, h, o);
+  h.t = t0;
+  h.tEnd = 1e300;
+  h.dt = dts[0];
+  h.cur = c->cur;
+  h.frozen = 1;
+  h.dtList = c->dtList;
+  h.nList = n;
+  h.rhsEvals = 1;
+  if (int rc = run_loop(c)) return rc;
+  if (h.done == 3) return fail(c, SGNB_ERR_NAN, "non-finite state");
+  return SGNB_OK;
+}
+
+static int diag(sgnb_ctx* c, int what, double* out) {
+  if (!c || !out) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  SGNB_CU(c, dev::launch_reduce_diag(what, c->C, c->U[c->cur], c->tab.qw, c->diag, c->ndiag, c->stream));
+  std::vector<double> part(c->ndiag);
+  SGNB_CU(c, cudaMemcpyAsync(part.data(), c->diag, c->ndiag * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  double acc = 0.0;
+  for (double v : part) acc = (what == 0) ? std::fmax(acc, v) : acc + v;
+  *out = acc;
+  return SGNB_OK;
+}
+
+int sgnb_max_wave_speed(sgnb_ctx* c, double* out) { return diag(c, 0, out); }
+
+int sgnb_cfl_time_step(sgnb_ctx* c, double cfl, double* out) {
+  double lam = 0.0;
+  if (int rc = diag(c, 0, &lam)) return rc;
+  // SGN2D::cflTimeStep (sgn2d.cpp:310-314)
+  const double dxEff = std::fmin(c->mesh.hx, c->mesh.hy) / (2.0 * c->desc.P + 1.0);
+  *out = cfl * dxEff / (lam > 0.0 ? lam : 1e-300);
+  return SGNB_OK;
+}
+
+int sgnb_mass(sgnb_ctx* c, double* out) {
+  double m = 0.0;
+  if (int rc = diag(c, 1, &m)) return rc;
+  *out = m * (c->C.Jx * c->C.Jy);
+  return SGNB_OK;
+}
+
+int sgnb_energy(sgnb_ctx* c, double* out) {
+  double E = 0.0;
+  if (int rc = diag(c, 2, &E)) return rc;
+  *out = E * (c->C.Jx * c->C.Jy);
+  return SGNB_OK;
+}
+
+int sgnb_node_coords(const sgnb_ctx* c, double* x, double* y) {
+  if (!c || !x || !y) return SGNB_ERR_INVALID;
+  node_coords(c->mesh, c->tab, x, y);
+  return SGNB_OK;
+}
+
+int sgnb_attempt_log(sgnb_ctx* c, double* out, long long cap, long long* n) {
+  if (!c || (cap > 0 && !out)) return fail(c, SGNB_ERR_INVALID, "bad arguments");
+  if (int rc = set_device(c)) return rc;
+  const long long have = c->hctrl->attempts < sgnb_ctx::kLogCap ? c->hctrl->attempts : sgnb_ctx::kLogCap;
+  const long long m = have < cap ? have : cap;
+  if (m > 0)
+    SGNB_CU(c, cudaMemcpy(out, c->alog, 4 * m * sizeof(double), cudaMemcpyDeviceToHost));
+  if (n) *n = have;
+  return SGNB_OK;
+}
+
+int sgnb_state_device_ptr(sgnb_ctx* c, double** U, void** stream) {
+  if (!c) return SGNB_ERR_INVALID;
+  if (U) *U = c->U[c->cur];
+  if (stream) *stream = (void*)c->stream;
+  return SGNB_OK;
+}
+
+const char* sgnb_status_string(int s) {
+  switch (s) {
+    case SGNB_OK: return "ok";
+    case SGNB_ERR_INVALID: return "invalid argument";
+    case SGNB_ERR_UNSUPPORTED: return "unsupported configuration";
+    case SGNB_ERR_CUDA: return "CUDA error";
+    case SGNB_ERR_NAN: return "non-finite state";
+    case SGNB_ERR_DTMIN: return "step size below dtMin";
+    case SGNB_ERR_TIMEOUT: return "device wait timed out";
+    case SGNB_ERR_NOMEM: return "out of device memory";
+    case SGNB_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* sgnb_last_error(const sgnb_ctx* c) {
+  return c ? c->err.c_str() : g_create_error.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// sgnb_device.h -- parameter blocks shared by the host code and the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sgnb {
+
+// Everything the fused right-hand-side kernel needs besides the state: mesh size,
+// boundary kinds, the physical constants in the exact forms the reference multiplies
+// them in (src/physics/sgn_flux2d.h:89-161), the FR tables, and the bathymetry statics.
+struct RhsConsts {
+  int Nx, Ny;          // elements per direction
+  int bcx, bcy;        // 0 periodic, 1 reflective wall
+  long long Nd;        // nodes per field = 25 Nx Ny
+  double g;            // gravity
+  double halfg;        // 0.5 * g
+  double gamma;        // dispersion parameter
+  double c2;           // c * c
+  double mc2;          // (-c) * c, the ncp coefficient
+  double m2c2;         // -2.0 * c2, the relaxation-source coefficient
+  double Jx, Jy;       // affine Jacobians hx/2, hy/2
+  double iJx, iJy;     // 1/Jx, 1/Jy (fast mode)
+  double D[25];        // GLL differentiation matrix, row-major
+  double gLp[5], gRp[5];  // g_DG correction derivatives
+  // bathymetry statics (device pointers)
+  const double* Hnod;    // nodal H, Nd
+  const double* Hx;      // nodal dH/dx, Nd
+  const double* Hy;      // nodal dH/dy, Nd
+  const double* HfX;     // H at the left edge of each element, 5 per element
+  const double* HfY;     // H at the bottom edge of each element
+  const double* HfXEnd;  // H on the right domain edge (walls), 5 per row
+  const double* HfYEnd;  // H on the top domain edge (walls), 5 per column
+};
+
+// Device-resident state of the adaptive integrator: the scalar loop variables of
+// src/solver/rk.cpp:67-164 plus the index of the buffer pair that holds u and k1.
+struct CtrlState {
+  double t, dt, tEnd, errPrev;
+  double tReached, dtLast, maxNormLast, errLast;
+  long long accepted, rejected, rhsEvals, attempts;
+  int cur;     // U[cur] holds u, K1[cur] holds k1
+  int done;    // 0 running, 1 reached tEnd, 2 dt fell below dtMin, 3 non-finite error
+  int frozen;  // 1: replay the dt list (every attempt accepted)
+  int pad;
+  double atol, rtol, dtMin, dtMax, safety, facMin, facMax, alpha, beta;
+  const double* dtList;  // frozen-dt replay list
+  long long nList;
+  double* log;           // attempt log: (t, dt, errNorm, accepted) per attempt
+  long long logCap;      // capacity of the log in attempts
+};
+
+// Buffers of one fused launch.
+struct StageArgs {
+  const double* in;   // MODE_RHS input state
+  double* out;        // MODE_RHS / MODE_STAGE output derivative
+  double* U[2];       // state ping-pong pair
+  double* K1[2];      // k1 / k4 ping-pong pair
+  double* K2;
+  double* K3;
+  int kin_k2;         // MODE_STAGE: add k2 (1) or k1 = K1[cur] (0) to u
+  double coef;        // MODE_STAGE: 0.5 or 0.75
+  const CtrlState* ctrl;
+  double* partials;   // MODE_FSAL: 3 doubles per CTA (sum r^2, max |r|, NaN count)
+};
+
+namespace dev {
+// Launchers (one translation unit per arithmetic mode).
+cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
+                               cudaStream_t s);
+cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A,
+                              cudaStream_t s);
+cudaError_t prepare_fused_exact();
+cudaError_t prepare_fused_fast();
+int fused_grid_blocks(int Nx, int Ny);
+size_t fused_smem_bytes();
+
+// Controller of one adaptive attempt: deterministic reduction of the per-CTA error
+// partials, accept/reject, PI step-size update and the next attempt's dt.
+cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk,
+                              long long n, cudaStream_t s);
+// Reductions over the uploaded state (diagnostics).
+cudaError_t launch_reduce_diag(int what, const RhsConsts& C, const double* U,
+                               const double* qw, double* out_partials, int nblk,
+                               cudaStream_t s);
+}  // namespace dev
+
+}  // namespace sgnb

@@ -1,0 +1,16 @@
+// sgnb_kernels_exact.cu -- fused kernels in the exact arithmetic mode.
+// Built with -fmad=false: every product and sum rounds separately, in the operation
+// order of the reference CPU solver, so the results are bit-identical to it.
+#define SGNB_EXACT true
+#include "sgnb_kernels_inst.cuh"
+
+namespace sgnb {
+namespace dev {
+cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
+  return launch_any(mode, C, A, s);
+}
+cudaError_t prepare_fused_exact() { return prepare_all(); }
+int fused_grid_blocks(int Nx, int Ny) { return ((Nx + TX - 1) / TX) * ((Ny + TY - 1) / TY); }
+size_t fused_smem_bytes() { return sizeof(Smem); }
+}  // namespace dev
+}  // namespace sgnb

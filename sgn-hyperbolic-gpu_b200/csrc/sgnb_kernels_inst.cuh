@@ -1,0 +1,41 @@
+// sgnb_kernels_inst.cuh -- instantiates the fused kernels for one arithmetic mode.
+// Included by sgnb_kernels_exact.cu (SGNB_EXACT = true, built with -fmad=false) and
+// sgnb_kernels_fast.cu (SGNB_EXACT = false, built with -fmad=true).
+#pragma once
+
+#include "sgnb_kernels.cuh"
+
+namespace sgnb {
+namespace dev {
+
+template <int MODE>
+static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
+  const dim3 grid((C.Nx + TX - 1) / TX, (C.Ny + TY - 1) / TY);
+  k_fused<MODE, SGNB_EXACT><<<grid, NTHR, sizeof(Smem), s>>>(C, A);
+  return cudaGetLastError();
+}
+
+static cudaError_t prepare_all() {
+  const int bytes = (int)sizeof(Smem);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+static cudaError_t launch_any(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
+  switch (mode) {
+    case MODE_RHS: return launch_mode<MODE_RHS>(C, A, s);
+    case MODE_STAGE: return launch_mode<MODE_STAGE>(C, A, s);
+    case MODE_FSAL: return launch_mode<MODE_FSAL>(C, A, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace dev
+}  // namespace sgnb

@@ -1,0 +1,160 @@
+// sgnb_rk.cu -- device-side controller of the adaptive Bogacki-Shampine 3(2) loop and
+// the diagnostic reductions. Built with -fmad=false: the controller arithmetic follows
+// src/solver/rk.cpp:112-161 operation for operation.
+#include "sgnb_device.h"
+
+#include <cmath>
+
+namespace sgnb {
+namespace dev {
+
+namespace {
+
+constexpr int kCtrlThreads = 256;
+
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+
+// One adaptive attempt has just written its per-CTA error partials. Reduce them in a
+// fixed order (so reruns are bit-reproducible), then apply the reference controller:
+// accept if the RMS scaled error <= 1 (rk.cpp:129-142), PI update clamped to
+// [facMin, facMax] (:148-152), dtMin abort (:155-160), and the loop test and the
+// end-time clip of the next attempt (:95-97).
+__global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const double* partials,
+                                                             int nblk, long long n) {
+  __shared__ double ss[kCtrlThreads], sm[kCtrlThreads], sn[kCtrlThreads];
+  if (c->done) return;
+  const int t = threadIdx.x;
+  double s = 0.0, m = 0.0, nn = 0.0;
+  for (int b = t; b < nblk; b += kCtrlThreads) {
+    s += partials[3 * b + 0];
+    m = dmax(m, partials[3 * b + 1]);
+    nn += partials[3 * b + 2];
+  }
+  ss[t] = s;
+  sm[t] = m;
+  sn[t] = nn;
+  __syncthreads();
+  for (int off = kCtrlThreads / 2; off > 0; off >>= 1) {
+    if (t < off) {
+      ss[t] += ss[t + off];
+      sm[t] = dmax(sm[t], sm[t + off]);
+      sn[t] += sn[t + off];
+    }
+    __syncthreads();
+  }
+  if (t != 0) return;
+  const double errL2 = sqrt(ss[0] / (double)n);
+  const double errMax = sm[0];
+  const double errNorm = dmax(errL2, 1e-300);
+  const bool bad = (sn[0] > 0.0) || (errNorm != errNorm);
+  if (c->log && c->attempts < c->logCap) {
+    double* row = c->log + 4 * c->attempts;
+    row[0] = c->t;
+    row[1] = c->dt;
+    row[2] = errNorm;
+    row[3] = (c->frozen || errNorm <= 1.0) ? 1.0 : 0.0;
+  }
+  c->attempts += 1;
+  c->rhsEvals += 3;
+  c->errLast = errNorm;
+  if (c->frozen) {  // replay of a given dt sequence: every step is taken
+    c->t += c->dt;
+    c->cur ^= 1;
+    c->accepted += 1;
+    c->tReached = c->t;
+    c->dtLast = c->dt;
+    c->maxNormLast = errMax;
+    if (bad) { c->done = 3; return; }
+    if (c->accepted >= c->nList) { c->done = 1; return; }
+    c->dt = c->dtList[c->accepted];
+    return;
+  }
+  if (errNorm <= 1.0) {
+    c->t += c->dt;
+    c->cur ^= 1;  // uNew becomes u and k4 becomes k1 (FSAL)
+    c->accepted += 1;
+    c->tReached = c->t;
+    c->dtLast = c->dt;
+    c->maxNormLast = errMax;
+    c->errPrev = errNorm;
+  } else {
+    c->rejected += 1;
+  }
+  if (bad) { c->done = 3; return; }  // the reference would loop forever here
+  double fac = c->safety * pow(errNorm, -c->alpha) * pow(c->errPrev, c->beta);
+  fac = (fac < c->facMin) ? c->facMin : ((c->facMax < fac) ? c->facMax : fac);
+  double dtNext = c->dt * fac;
+  dtNext = dmin(dtNext, c->dtMax);
+  if (dtNext < c->dtMin) {
+    c->done = 2;
+    c->dtLast = dtNext;
+    return;
+  }
+  c->dt = dtNext;
+  const double tEnd = c->tEnd;
+  if (!(c->t < tEnd - 1e-15 * dmax(1.0, fabs(tEnd)))) { c->done = 1; return; }
+  if (c->t + c->dt > tEnd) c->dt = tEnd - c->t;
+}
+
+struct QW {
+  double w[5];
+};
+
+// Per-block reductions over the nodes of a state: what = 0 largest characteristic
+// speed (SGN2D::maxWaveSpeed, src/solver/sgn2d.cpp:295-305), 1 mass (:319-329),
+// 2 energy (:334-348). Each block writes one partial; the host combines them.
+__global__ void __launch_bounds__(256) k_diag(int what, const RhsConsts C, const double* U,
+                                              const QW q, double* out) {
+  __shared__ double sh[256];
+  const long long Nd = C.Nd;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < Nd;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double h = U[i], hu = U[Nd + i], hv = U[2 * Nd + i];
+    const int loc = (int)(i % 25);
+    const double wq = q.w[loc % 5] * q.w[loc / 5];
+    if (what == 0) {
+      const double p = U[4 * Nd + i] / h;
+      const double arg = C.g * h + p + C.c2;
+      const double ce = sqrt(arg > 0.0 ? arg : 0.0);
+      const double lx = fabs(hu / h) + ce, ly = fabs(hv / h) + ce;
+      acc = fmax(acc, fmax(lx, ly));
+    } else if (what == 1) {
+      acc += wq * h;
+    } else {
+      const double u = hu / h, v = hv / h, w = U[3 * Nd + i] / h;
+      const double e = 0.5 * h * (u * u + v * v + (1.0 / C.gamma) * w * w +
+                                  C.g * (h - 2.0 * C.Hnod[i]));
+      acc += wq * e;
+    }
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if (threadIdx.x < off)
+      sh[threadIdx.x] = (what == 0) ? fmax(sh[threadIdx.x], sh[threadIdx.x + off])
+                                    : sh[threadIdx.x] + sh[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+}  // namespace
+
+cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk, long long n,
+                              cudaStream_t s) {
+  k_controller<<<1, kCtrlThreads, 0, s>>>(c, partials, nblk, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_diag(int what, const RhsConsts& C, const double* U, const double* qw,
+                               double* out_partials, int nblk, cudaStream_t s) {
+  QW q;
+  for (int k = 0; k < 5; ++k) q.w[k] = qw[k];
+  k_diag<<<nblk, 256, 0, s>>>(what, C, U, q, out_partials);
+  return cudaGetLastError();
+}
+
+}  // namespace dev
+}  // namespace sgnb

@@ -1,0 +1,33 @@
+// sgnb_setup.h -- host-side set-up: FR tables, node coordinates, bathymetry statics.
+#pragma once
+
+#include <vector>
+
+namespace sgnb {
+
+// FROperators1D for GLL points (src/core/fr_operators.h:57-115), degree P <= 7.
+struct FrTables {
+  int P = 0;
+  double nodes[8] = {}, D[64] = {}, lL[8] = {}, lR[8] = {}, gLp[8] = {}, gRp[8] = {}, qw[8] = {};
+};
+
+// CartesianMesh2D geometry (src/core/mesh2d.h:23-51).
+struct Mesh {
+  int Nx = 0, Ny = 0;
+  double Lx = 0, Ly = 0, hx = 0, hy = 0;
+};
+
+// Bathymetry statics read by the kernels (SGN2D accessors, src/solver/sgn2d.h:94-98),
+// plus the depth on the right / top domain edges used by walls.
+struct Bathymetry {
+  std::vector<double> Hnod, Hx, Hy, HfX, HfY, HfXEnd, HfYEnd;
+};
+
+bool fr_tables(int P, FrTables& t);
+double still_depth(int kind, const double* p, double x, double y);
+// number of doubles a parameter vector of this kind must hold (-1: unknown kind)
+int bathy_param_count(int kind, const double* p, int n);
+void node_coords(const Mesh& m, const FrTables& t, double* x, double* y);
+void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p, Bathymetry& out);
+
+}  // namespace sgnb
