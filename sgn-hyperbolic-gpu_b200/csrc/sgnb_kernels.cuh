@@ -65,29 +65,56 @@ struct Smem {
   double Hx[TE][NPP];          // nodal dH/dx
   double Hy[TE][NPP];          // nodal dH/dy
   double G[NV + 1][TE][NPP];   // column-pass results dG (5 fields) and By; then dU
-  double haloL[NV][TY][NP];    // node (4,b) of the element left of the tile, per row
-  double haloR[NV][TY][NP];    // node (0,b) of the element right of the tile
-  double haloB[NV][TX][NP];    // node (a,4) of the element below the tile, per column
-  double haloT[NV][TX][NP];    // node (a,0) of the element above the tile
-  double HfX[TE][NP];          // left-edge depth of each tile element
-  double HfY[TE][NP];          // bottom-edge depth
-  double HfXR[TY][NP];         // right-edge depth of the last tile column, per row
-  double HfYT[TX][NP];         // top-edge depth of the last tile row, per column
+  // halo node states, flat index q = t + NP * (slot + NHALO * v):
+  //   slot 0..TY-1        node (4,t) of the element left of tile row slot
+  //   slot TY..2TY-1      node (0,t) of the element right of tile row slot-TY
+  //   slot 2TY..2TY+TX-1  node (t,4) of the element below tile column slot-2TY
+  //   slot 2TY+TX..       node (t,0) of the element above tile column slot-2TY-TX
+  double halo[NV * (2 * TY + 2 * TX) * NP];
+  // face depths, flat: HfX[TE][NP] (left edges), HfY[TE][NP] (bottom edges),
+  // HfXR[TY][NP] (right edge of the last tile column), HfYT[TX][NP] (top edge of the
+  // last tile row)
+  double Hf[(2 * TE + TY + TX) * NP];
   double red[NWARP][3];        // block reduction of the error partials
+};
+
+constexpr int NHALO = 2 * TY + 2 * TX;                 // halo slots per field
+constexpr int RUN = TX * NPP;                          // doubles per tile row and field
+constexpr int NIT = TY * RUN / NTHR;                   // own-node items per thread
+static_assert(TY * RUN == NIT * NTHR, "own nodes split evenly over the threads");
+constexpr int NHIT = (NV * NHALO * NP + NTHR - 1) / NTHR;          // halo items per thread
+constexpr int NFACE = (2 * TE + TY + TX) * NP;
+constexpr int NFIT = (NFACE + NTHR - 1) / NTHR;                    // face-depth items
+
+__device__ __forceinline__ double& hf_x(Smem& S, int i, int t) { return S.Hf[i * NP + t]; }
+__device__ __forceinline__ double& hf_y(Smem& S, int i, int t) { return S.Hf[(TE + i) * NP + t]; }
+__device__ __forceinline__ double& hf_xr(Smem& S, int iy, int t) { return S.Hf[(2 * TE + iy) * NP + t]; }
+__device__ __forceinline__ double& hf_yt(Smem& S, int ix, int t) { return S.Hf[(2 * TE + TY + ix) * NP + t]; }
+__device__ __forceinline__ double& halo_at(Smem& S, int v, int slot, int t) {
+  return S.halo[t + NP * (slot + NHALO * v)];
+}
+
+// Read-only views of the stage inputs of one launch.
+struct StageIn {
+  const double* __restrict__ in;
+  const double* __restrict__ u;
+  const double* __restrict__ k;   // MODE_STAGE: the derivative added to u
+  const double* __restrict__ k1;
+  const double* __restrict__ k2;
+  const double* __restrict__ k3;
+  double acoef, dt;
 };
 
 // Stage input of one value: plain, u + (coef dt) k, or the BS3 candidate.
 // Expression trees follow src/solver/rk.cpp:100-108 exactly.
 template <int MODE>
-__device__ __forceinline__ double stage_value(const StageArgs& A, int cur, double dt,
-                                              double acoef, long long idx) {
+__device__ __forceinline__ double stage_value(const StageIn& I, long long idx) {
   if constexpr (MODE == MODE_RHS) {
-    return A.in[idx];
+    return I.in[idx];
   } else if constexpr (MODE == MODE_STAGE) {
-    return A.U[cur][idx] + acoef * (A.kin_k2 ? A.K2 : A.K1[cur])[idx];
+    return I.u[idx] + I.acoef * I.k[idx];
   } else {
-    return A.U[cur][idx] + dt * (2.0 / 9.0 * A.K1[cur][idx] + 1.0 / 3.0 * A.K2[idx] +
-                                 4.0 / 9.0 * A.K3[idx]);
+    return I.u[idx] + I.dt * (2.0 / 9.0 * I.k1[idx] + 1.0 / 3.0 * I.k2[idx] + 4.0 / 9.0 * I.k3[idx]);
   }
 }
 
@@ -99,35 +126,63 @@ __device__ __forceinline__ double canon(double v) {
   if constexpr (EXACT) return v + 0.0; else return v;
 }
 
+// Reciprocal for the fast mode: the hardware estimate (PTX rcp.approx.ftz.f64) refined by
+// two Newton-Raphson steps r <- r + r (1 - x r), each of which doubles the number of
+// correct bits. Accurate to a few ulp for the positive normal depths it is used on; the
+// library's self-test compares it with IEEE 1/x.
+__device__ __forceinline__ double fast_rcp(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  return r;
+}
+
 // Primitive variables u, v, w, p of one point (src/physics/sgn_flux2d.h:92-93).
 template <bool EXACT>
 struct Prim {
   double u, v, w, p;
-  __device__ __forceinline__ Prim(const double* U) {
+  __device__ __forceinline__ Prim() {}
+  __device__ __forceinline__ explicit Prim(const double* U) {
     if constexpr (EXACT) {
       u = U[1] / U[0]; v = U[2] / U[0]; w = U[3] / U[0]; p = U[4] / U[0];
     } else {
-      const double ih = 1.0 / U[0];
+      const double ih = fast_rcp(U[0]);
       u = U[1] * ih; v = U[2] * ih; w = U[3] * ih; p = U[4] * ih;
     }
   }
 };
 
+// Hydrostatic part 0.5 g (h^2 - H^2) of the normal momentum flux. h^2 - H^2 cancels
+// where h ~ H; both modes round the two squares separately, as the CPU does, because
+// the derivative amplifies this term's rounding by ~|D|/J.
+__device__ __forceinline__ double hydro(const RhsConsts& C, double h, double Hloc) {
+  return C.halfg * (__dmul_rn(h, h) - __dmul_rn(Hloc, Hloc));
+}
+
+// Normal-momentum component of the directional flux (sgn_flux2d.h:94, 109).
+template <bool EXACT, int DIR>
+__device__ __forceinline__ double flux_normal(const RhsConsts& C, const double* U,
+                                              const Prim<EXACT>& q, double Hloc) {
+  const double hn = DIR == 0 ? U[1] : U[2];
+  const double hp = EXACT ? U[0] * q.p : U[4];
+  return hn * (DIR == 0 ? q.u : q.v) + hydro(C, U[0], Hloc) + hp;
+}
+
 // Directional flux: fluxX (DIR 0) or fluxY (DIR 1), src/physics/sgn_flux2d.h:89-116.
 template <bool EXACT, int DIR>
 __device__ __forceinline__ void flux(const RhsConsts& C, const double* U, const Prim<EXACT>& q,
                                      double Hloc, double* F) {
-  const double h = U[0];
   const double hn = DIR == 0 ? U[1] : U[2];  // normal discharge
-  const double hyd = C.halfg * (h * h - Hloc * Hloc);
-  const double hp = EXACT ? h * q.p : U[4];
   F[0] = hn;
   if constexpr (DIR == 0) {
-    F[1] = hn * q.u + hyd + hp;
+    F[1] = flux_normal<EXACT, DIR>(C, U, q, Hloc);
     F[2] = hn * q.v;
   } else {
     F[1] = hn * q.u;
-    F[2] = hn * q.v + hyd + hp;
+    F[2] = flux_normal<EXACT, DIR>(C, U, q, Hloc);
   }
   F[3] = hn * q.w;
   F[4] = hn * (q.p + C.c2);
@@ -142,34 +197,47 @@ __device__ __forceinline__ double wave_speed(const RhsConsts& C, const double* U
   return fabs(DIR == 0 ? q.u : q.v) + ce;
 }
 
-// Results of one GLL line (5 nodes) in one direction.
-struct LineOut {
-  double d[NP][NV];  // FR-corrected flux derivative of each node, /J
-  double dh[NP];     // FR-corrected depth derivative of each node, /J
-};
+// Field v of the directional flux from the per-node quantities: normal discharge hn,
+// primitives q and the precomputed normal-momentum component fn (sgn_flux2d.h:89-116).
+template <bool EXACT, int DIR>
+__device__ __forceinline__ double flux_field(const RhsConsts& C, int v, double hn,
+                                             const Prim<EXACT>& q, double fn) {
+  switch (v) {
+    case 0: return hn;
+    case 1: return DIR == 0 ? fn : hn * q.u;
+    case 2: return DIR == 0 ? hn * q.v : fn;
+    case 3: return hn * q.w;
+    default: return hn * (q.p + C.c2);
+  }
+}
 
-// The line computation shared by the row (DIR 0) and column (DIR 1) passes:
-// nodal fluxes, both Rusanov face fluxes with central depths, the element's own
-// face fluxes, the 5-point differentiation and the correction lift
-// (src/solver/sgn2d.cpp:188-275 restricted to one line).
+// The line computation shared by the row (DIR 0) and column (DIR 1) passes: nodal
+// fluxes, both Rusanov face fluxes with central depths, the element's own face fluxes,
+// the 5-point differentiation and the correction lift (src/solver/sgn2d.cpp:188-275
+// restricted to one line).
 //   Un[k]   raw node states along the line, k = 0..4 (low face at k = 0)
 //   Hn[k]   nodal still depth
 //   nLo/nHi raw node state of the neighbour across the low/high face (or the mirror
 //           ghost at a wall)
 //   HfLo/HfHi still depth at the two faces
-template <bool EXACT, int DIR>
+// Results go out through two callbacks: emit_dh(m, dh, q) with the FR-corrected depth
+// derivative of node m, then emit(m, v, d, q) with the FR-corrected derivative of flux
+// field v at node m (both already divided by J). The flux of each field is rebuilt from
+// per-node quantities inside the contraction, which keeps the live set small.
+template <bool EXACT, int DIR, class EmitH, class Emit>
 __device__ __forceinline__ void line_pass(const RhsConsts& C, const double (&Un)[NP][NV],
                                           const double (&Hn)[NP], const double* nLo,
                                           const double* nHi, double HfLo, double HfHi,
-                                          LineOut& out) {
-  // nodal fluxes
-  double F[NP][NV];
+                                          EmitH&& emit_dh, Emit&& emit) {
+  Prim<EXACT> q[NP];
+  double hn[NP], fn[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    const Prim<EXACT> q(Un[k]);
-    flux<EXACT, DIR>(C, Un[k], q, Hn[k], F[k]);
+    q[k] = Prim<EXACT>(Un[k]);
+    hn[k] = DIR == 0 ? Un[k][1] : Un[k][2];
+    fn[k] = flux_normal<EXACT, DIR>(C, Un[k], q[k], Hn[k]);
   }
-  // face traces (own side and the neighbour side)
+  // face traces: own side t*, neighbour side s*
   double tLo[NV], tHi[NV], sLo[NV], sHi[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
@@ -178,58 +246,86 @@ __device__ __forceinline__ void line_pass(const RhsConsts& C, const double (&Un)
     sLo[v] = canon<EXACT>(nLo[v]);
     sHi[v] = canon<EXACT>(nHi[v]);
   }
-  const Prim<EXACT> qtLo(tLo), qtHi(tHi), qsLo(sLo), qsHi(sHi);
-  // own face fluxes Fd (sgn2d.cpp:229-239) and the neighbours' fluxes at the faces
-  double FdLo[NV], FdHi[NV], FnLo[NV], FnHi[NV];
-  flux<EXACT, DIR>(C, tLo, qtLo, HfLo, FdLo);
-  flux<EXACT, DIR>(C, tHi, qtHi, HfHi, FdHi);
-  flux<EXACT, DIR>(C, sLo, qsLo, HfLo, FnLo);
-  flux<EXACT, DIR>(C, sHi, qsHi, HfHi, FnHi);
-  // Rusanov (sgn_flux2d.h:169-179); the low face has the neighbour on its left
-  const double lamLo = fmax(wave_speed<EXACT, DIR>(C, sLo, qsLo), wave_speed<EXACT, DIR>(C, tLo, qtLo));
-  const double lamHi = fmax(wave_speed<EXACT, DIR>(C, tHi, qtHi), wave_speed<EXACT, DIR>(C, sHi, qsHi));
   double jLo[NV], jHi[NV];  // common flux minus own face flux
-#pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    const double fsLo = 0.5 * (FnLo[v] + FdLo[v]) - 0.5 * lamLo * (tLo[v] - sLo[v]);
-    const double fsHi = 0.5 * (FdHi[v] + FnHi[v]) - 0.5 * lamHi * (sHi[v] - tHi[v]);
-    jLo[v] = fsLo - FdLo[v];
-    jHi[v] = fsHi - FdHi[v];
-  }
-  // central common depth h* and its jump (sgn2d.cpp:213-214, 271-274)
-  const double jhLo = 0.5 * (sLo[0] + tLo[0]) - tLo[0];
-  const double jhHi = 0.5 * (tHi[0] + sHi[0]) - tHi[0];
-#pragma unroll
-  for (int m = 0; m < NP; ++m) {
+  {
+    const Prim<EXACT> qsLo(sLo), qsHi(sHi);
+    Prim<EXACT> qtLo, qtHi;
+    if constexpr (EXACT) {
+      qtLo = Prim<EXACT>(tLo);
+      qtHi = Prim<EXACT>(tHi);
+    } else {
+      qtLo = q[0];
+      qtHi = q[NP - 1];
+    }
+    const double fnLo_t = flux_normal<EXACT, DIR>(C, tLo, qtLo, HfLo);
+    const double fnHi_t = flux_normal<EXACT, DIR>(C, tHi, qtHi, HfHi);
+    const double fnLo_s = flux_normal<EXACT, DIR>(C, sLo, qsLo, HfLo);
+    const double fnHi_s = flux_normal<EXACT, DIR>(C, sHi, qsHi, HfHi);
+    const double hnLo_t = tLo[1 + DIR], hnHi_t = tHi[1 + DIR];
+    const double hnLo_s = sLo[1 + DIR], hnHi_s = sHi[1 + DIR];
+    // Rusanov (sgn_flux2d.h:169-179); the low face has the neighbour on its left
+    const double lamLo = fmax(wave_speed<EXACT, DIR>(C, sLo, qsLo), wave_speed<EXACT, DIR>(C, tLo, qtLo));
+    const double lamHi = fmax(wave_speed<EXACT, DIR>(C, tHi, qtHi), wave_speed<EXACT, DIR>(C, sHi, qsHi));
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
+      // own face flux Fd (sgn2d.cpp:229-239) and the neighbour's flux at the face
+      const double FdLo = flux_field<EXACT, DIR>(C, v, hnLo_t, qtLo, fnLo_t);
+      const double FdHi = flux_field<EXACT, DIR>(C, v, hnHi_t, qtHi, fnHi_t);
+      const double FnLo = flux_field<EXACT, DIR>(C, v, hnLo_s, qsLo, fnLo_s);
+      const double FnHi = flux_field<EXACT, DIR>(C, v, hnHi_s, qsHi, fnHi_s);
+      const double fsLo = 0.5 * (FnLo + FdLo) - 0.5 * lamLo * (tLo[v] - sLo[v]);
+      const double fsHi = 0.5 * (FdHi + FnHi) - 0.5 * lamHi * (sHi[v] - tHi[v]);
+      jLo[v] = fsLo - FdLo;
+      jHi[v] = fsHi - FdHi;
+    }
+  }
+  // FR-corrected depth derivative with the central common depth h* (sgn2d.cpp:265-275)
+  {
+    const double jhLo = 0.5 * (sLo[0] + tLo[0]) - tLo[0];
+    const double jhHi = 0.5 * (tHi[0] + sHi[0]) - tHi[0];
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+      double dh;
       if constexpr (EXACT) {
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) s += C.D[m * NP + k] * F[k][v];
+        for (int k = 0; k < NP; ++k) s += C.D[m * NP + k] * Un[k][0];
+        s += jhLo * C.gLp[m] + jhHi * C.gRp[m];
+        dh = s / (DIR == 0 ? C.Jx : C.Jy);
+      } else {
+        double s = jhLo * C.gLp[m];
+        s = fma(jhHi, C.gRp[m], s);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) s = fma(C.D[m * NP + k], Un[k][0], s);
+        dh = s * (DIR == 0 ? C.iJx : C.iJy);
+      }
+      emit_dh(m, dh, q[m]);
+    }
+  }
+  // FR-corrected flux divergence, field by field (sgn2d.cpp:248-263)
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double F[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) F[k] = flux_field<EXACT, DIR>(C, v, hn[k], q[k], fn[k]);
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+      double d;
+      if constexpr (EXACT) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) s += C.D[m * NP + k] * F[k];
         const double c = jLo[v] * C.gLp[m] + jHi[v] * C.gRp[m];
-        out.d[m][v] = (s + c) / (DIR == 0 ? C.Jx : C.Jy);
+        d = (s + c) / (DIR == 0 ? C.Jx : C.Jy);
       } else {
         // accumulate with the unscaled tables, one rounding for 1/J at the end
         double s = jLo[v] * C.gLp[m];
         s = fma(jHi[v], C.gRp[m], s);
 #pragma unroll
-        for (int k = 0; k < NP; ++k) s = fma(C.D[m * NP + k], F[k][v], s);
-        out.d[m][v] = s * (DIR == 0 ? C.iJx : C.iJy);
+        for (int k = 0; k < NP; ++k) s = fma(C.D[m * NP + k], F[k], s);
+        d = s * (DIR == 0 ? C.iJx : C.iJy);
       }
-    }
-    if constexpr (EXACT) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k < NP; ++k) s += C.D[m * NP + k] * Un[k][0];
-      s += jhLo * C.gLp[m] + jhHi * C.gRp[m];
-      out.dh[m] = s / (DIR == 0 ? C.Jx : C.Jy);
-    } else {
-      double s = jhLo * C.gLp[m];
-      s = fma(jhHi, C.gRp[m], s);
-#pragma unroll
-      for (int k = 0; k < NP; ++k) s = fma(C.D[m * NP + k], Un[k][0], s);
-      out.dh[m] = s * (DIR == 0 ? C.iJx : C.iJy);
+      emit(m, v, d, q[m]);
     }
   }
 }
@@ -242,8 +338,6 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
   ghost[DIR == 0 ? 1 : 2] = -own[DIR == 0 ? 1 : 2];
 }
 
-__device__ __forceinline__ bool spin_ok(long long& n) { return ++n < (1ll << 40); }
-
 template <int MODE, bool EXACT>
 __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -251,15 +345,24 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
 
   // ---- controller state (stage modes only) ---------------------------------
   int cur = 0;
-  double dt = 0.0, acoef = 0.0, atol = 0.0, rtol = 0.0;
+  double atol = 0.0, rtol = 0.0;
+  StageIn I;
+  I.in = A.in;
+  I.dt = 0.0;
+  I.acoef = 0.0;
   if constexpr (MODE != MODE_RHS) {
     if (A.ctrl->done) return;  // uniform across the grid
     cur = A.ctrl->cur;
-    dt = A.ctrl->dt;
-    acoef = A.coef * dt;  // 0.5 * dt or 0.75 * dt as in rk.cpp:100-103
+    I.dt = A.ctrl->dt;
+    I.acoef = A.coef * I.dt;  // 0.5 * dt or 0.75 * dt as in rk.cpp:100-103
     atol = A.ctrl->atol;
     rtol = A.ctrl->rtol;
   }
+  I.u = A.U[cur];
+  I.k = A.kin_k2 ? A.K2 : A.K1[cur];
+  I.k1 = A.K1[cur];
+  I.k2 = A.K2;
+  I.k3 = A.K3;
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -270,93 +373,132 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
   const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
   const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
 
-  // ---- load phase: tile state, statics and halos into shared memory --------
+  // ---- own-node item map: NIT items per thread, shared by every array -------
+  // item q = tid + NTHR*u is double k of tile row iy: global (e_row*25 + k), shared
+  // iy*RUN + k (the [TE][NPP] layout of one field). Recomputed after the passes rather
+  // than kept live through them.
+  long long gof[NIT];
+  int sof[NIT];
+  bool okk[NIT];
+  auto item_map = [&]() {
+#pragma unroll
+    for (int u = 0; u < NIT; ++u) {
+      const int q = tid + NTHR * u;
+      const int iy = q / RUN, k = q - iy * RUN;
+      okk[u] = iy < TYv && k < TXv * NPP;
+      gof[u] = ((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k;
+      sof[u] = iy * RUN + k;
+    }
+  };
+  item_map();
+
+  // ---- load phase --------------------------------------------------------------
   {
-    double* dstU = &S.U[0][0][0];
-    double* dstH = &S.H[0][0];
-    // own nodes: per field and tile row, TXv*25 contiguous doubles
-    for (int it = tid; it < NV * TY * TX * NPP; it += NTHR) {
-      const int k = it % (TX * NPP);
-      const int r = it / (TX * NPP);
-      const int iy = r % TY, v = r / TY;
-      if (iy >= TYv || k >= TXv * NPP) continue;
-      const long long eg = (long long)ex0 + (long long)Nx * (ey0 + iy);
-      const long long gi = (long long)v * Nd + eg * NPP + k;
-      const double val = stage_value<MODE>(A, cur, dt, acoef, gi);
-      dstU[(v * TE + iy * TX) * NPP + k] = val;
-      if constexpr (MODE == MODE_FSAL) A.U[cur ^ 1][gi] = val;
-    }
-    for (int it = tid; it < 3 * TY * TX * NPP; it += NTHR) {
-      const int k = it % (TX * NPP);
-      const int r = it / (TX * NPP);
-      const int iy = r % TY, s = r / TY;
-      if (iy >= TYv || k >= TXv * NPP) continue;
-      const long long eg = (long long)ex0 + (long long)Nx * (ey0 + iy);
-      const double* src = s == 0 ? C.Hnod : (s == 1 ? C.Hx : C.Hy);
-      dstH[(s * TE + iy * TX) * NPP + k] = src[eg * NPP + k];
-    }
-    // halos: left/right nodes per tile row, bottom/top nodes per tile column
-    for (int it = tid; it < NV * (2 * TY + 2 * TX) * NP; it += NTHR) {
-      const int t = it % NP;
-      const int r = it / NP;
-      const int slot = r % (2 * TY + 2 * TX), v = r / (2 * TY + 2 * TX);
-      long long e;
-      int node;
-      double* dst;
-      if (slot < TY) {  // left
-        const int iy = slot;
-        if (iy >= TYv || wallL) continue;
-        e = (long long)((ex0 - 1 + Nx) % Nx) + (long long)Nx * (ey0 + iy);
-        node = (NP - 1) + NP * t;
-        dst = &S.haloL[v][iy][t];
-      } else if (slot < 2 * TY) {  // right
-        const int iy = slot - TY;
-        if (iy >= TYv || wallR) continue;
-        e = (long long)((ex0 + TXv) % Nx) + (long long)Nx * (ey0 + iy);
-        node = NP * t;
-        dst = &S.haloR[v][iy][t];
-      } else if (slot < 2 * TY + TX) {  // bottom
-        const int ix = slot - 2 * TY;
-        if (ix >= TXv || wallB) continue;
-        e = (long long)(ex0 + ix) + (long long)Nx * ((ey0 - 1 + Ny) % Ny);
-        node = t + NP * (NP - 1);
-        dst = &S.haloB[v][ix][t];
-      } else {  // top
-        const int ix = slot - 2 * TY - TX;
-        if (ix >= TXv || wallT) continue;
-        e = (long long)(ex0 + ix) + (long long)Nx * ((ey0 + TYv) % Ny);
-        node = t;
-        dst = &S.haloT[v][ix][t];
+    // statics: all loads first, then the shared-memory stores
+    const double* __restrict__ gH = C.Hnod;
+    const double* __restrict__ gHx = C.Hx;
+    const double* __restrict__ gHy = C.Hy;
+    double a0[NIT], a1[NIT], a2[NIT];
+#pragma unroll
+    for (int u = 0; u < NIT; ++u)
+      if (okk[u]) { a0[u] = gH[gof[u]]; a1[u] = gHx[gof[u]]; a2[u] = gHy[gof[u]]; }
+    // statics to shared memory first: they are not needed in registers
+#pragma unroll
+    for (int u = 0; u < NIT; ++u)
+      if (okk[u]) {
+        (&S.H[0][0])[sof[u]] = a0[u];
+        (&S.Hx[0][0])[sof[u]] = a1[u];
+        (&S.Hy[0][0])[sof[u]] = a2[u];
       }
-      *dst = stage_value<MODE>(A, cur, dt, acoef, (long long)v * Nd + e * NPP + node);
+    // state: field by field, all items' loads of a field in flight together
+    double* __restrict__ unew = A.U[cur ^ 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double x[NIT];
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          (&S.U[v][0][0])[sof[u]] = x[u];
+          if constexpr (MODE == MODE_FSAL) unew[(long long)v * Nd + gof[u]] = x[u];
+        }
     }
-    // face depths
-    for (int it = tid; it < 2 * TE * NP + (TY + TX) * NP; it += NTHR) {
-      if (it < 2 * TE * NP) {
-        const int t = it % NP, i = (it / NP) % TE, s = it / (NP * TE);
-        const int ix = i % TX, iy = i / TX;
-        if (ix >= TXv || iy >= TYv) continue;
-        const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
-        if (s == 0) S.HfX[i][t] = C.HfX[e * NP + t];
-        else S.HfY[i][t] = C.HfY[e * NP + t];
+    // halo items: descriptors, then loads
+    double hv[NHIT];
+    int hq[NHIT];
+    long long hg[NHIT];
+#pragma unroll
+    for (int u = 0; u < NHIT; ++u) {
+      const int q = tid + NTHR * u;
+      const int t = q % NP, r = q / NP;
+      const int slot = r % NHALO, v = r / NHALO;
+      bool ok = q < NV * NHALO * NP;
+      long long e = 0;
+      int node = 0;
+      if (slot < TY) {
+        ok = ok && slot < TYv && !wallL;
+        e = (long long)((ex0 - 1 + Nx) % Nx) + (long long)Nx * (ey0 + slot);
+        node = (NP - 1) + NP * t;
+      } else if (slot < 2 * TY) {
+        ok = ok && slot - TY < TYv && !wallR;
+        e = (long long)((ex0 + TXv) % Nx) + (long long)Nx * (ey0 + slot - TY);
+        node = NP * t;
+      } else if (slot < 2 * TY + TX) {
+        ok = ok && slot - 2 * TY < TXv && !wallB;
+        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * ((ey0 - 1 + Ny) % Ny);
+        node = t + NP * (NP - 1);
       } else {
-        const int r = it - 2 * TE * NP;
+        ok = ok && slot - 2 * TY - TX < TXv && !wallT;
+        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * ((ey0 + TYv) % Ny);
+        node = t;
+      }
+      hq[u] = ok ? q : -1;
+      hg[u] = (long long)v * Nd + e * NPP + node;
+    }
+#pragma unroll
+    for (int u = 0; u < NHIT; ++u)
+      if (hq[u] >= 0) hv[u] = stage_value<MODE>(I, hg[u]);
+    // face depths
+    double fv[NFIT];
+    int fq[NFIT];
+#pragma unroll
+    for (int u = 0; u < NFIT; ++u) {
+      const int q = tid + NTHR * u;
+      fq[u] = -1;
+      if (q < 2 * TE * NP) {
+        const int t = q % NP, i = (q / NP) % TE, s = q / (NP * TE);
+        const int ix = i % TX, iy = i / TX;
+        if (ix < TXv && iy < TYv) {
+          const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
+          fv[u] = (s == 0 ? C.HfX : C.HfY)[e * NP + t];
+          fq[u] = q;
+        }
+      } else if (q < NFACE) {
+        const int r = q - 2 * TE * NP;
         const int t = r % NP, slot = r / NP;
         if (slot < TY) {
-          const int iy = slot;
-          if (iy >= TYv) continue;
-          const int ey = ey0 + iy;
-          S.HfXR[iy][t] = wallR ? C.HfXEnd[(long long)ey * NP + t]
-                                : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
-        } else {
-          const int ix = slot - TY;
-          if (ix >= TXv) continue;
-          const int ex = ex0 + ix;
-          S.HfYT[ix][t] = wallT ? C.HfYEnd[(long long)ex * NP + t]
-                                : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t];
+          if (slot < TYv) {
+            const int ey = ey0 + slot;
+            fv[u] = wallR ? C.HfXEnd[(long long)ey * NP + t]
+                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
+            fq[u] = q;
+          }
+        } else if (slot - TY < TXv) {
+          const int ex = ex0 + slot - TY;
+          fv[u] = wallT ? C.HfYEnd[(long long)ex * NP + t]
+                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t];
+          fq[u] = q;
         }
       }
     }
+#pragma unroll
+    for (int u = 0; u < NHIT; ++u)
+      if (hq[u] >= 0) S.halo[hq[u]] = hv[u];
+#pragma unroll
+    for (int u = 0; u < NFIT; ++u)
+      if (fq[u] >= 0) S.Hf[fq[u]] = fv[u];
   }
   __syncthreads();
 
@@ -382,7 +524,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<1>(Un[0], nLo);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nLo[v] = S.haloB[v][ix][j];
+      for (int v = 0; v < NV; ++v) nLo[v] = halo_at(S, v, 2 * TY + ix, j);
     }
     if (iy + 1 < TYv) {
 #pragma unroll
@@ -391,23 +533,16 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<1>(Un[NP - 1], nHi);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nHi[v] = S.haloT[v][ix][j];
+      for (int v = 0; v < NV; ++v) nHi[v] = halo_at(S, v, 2 * TY + TX + ix, j);
     }
-    const double HfLo = S.HfY[i][j];
-    const double HfHi = (iy + 1 < TYv) ? S.HfY[i + TX][j] : S.HfYT[ix][j];
-    LineOut lo;
-    line_pass<EXACT, 1>(C, Un, Hn, nLo, nHi, HfLo, HfHi, lo);
-#pragma unroll
-    for (int b = 0; b < NP; ++b) {
-      const int loc = j + NP * b;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) S.G[v][i][loc] = lo.d[b][v];
-      // ncpY (sgn_flux2d.h:156-161): -c^2 v h_y
-      double vv;
-      if constexpr (EXACT) vv = Un[b][2] / Un[b][0]; else vv = Un[b][2] * (1.0 / Un[b][0]);
-      const double hy = lo.dh[b];
-      S.G[NV][i][loc] = EXACT ? C.mc2 * vv * hy : C.mc2 * vv * hy;
-    }
+    const double HfLo = hf_y(S, i, j);
+    const double HfHi = (iy + 1 < TYv) ? hf_y(S, i + TX, j) : hf_yt(S, ix, j);
+    line_pass<EXACT, 1>(
+        C, Un, Hn, nLo, nHi, HfLo, HfHi,
+        [&](int b, double dh, const Prim<EXACT>& q) {
+          S.G[NV][i][j + NP * b] = C.mc2 * q.v * dh;  // ncpY (sgn_flux2d.h:156-161)
+        },
+        [&](int b, int v, double d, const Prim<EXACT>&) { S.G[v][i][j + NP * b] = d; });
   }
   __syncthreads();
 
@@ -430,7 +565,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<0>(Un[0], nLo);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nLo[v] = S.haloL[v][iy][j];
+      for (int v = 0; v < NV; ++v) nLo[v] = halo_at(S, v, iy, j);
     }
     if (ix + 1 < TXv) {
 #pragma unroll
@@ -439,75 +574,96 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<0>(Un[NP - 1], nHi);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nHi[v] = S.haloR[v][iy][j];
+      for (int v = 0; v < NV; ++v) nHi[v] = halo_at(S, v, TY + iy, j);
     }
-    const double HfLo = S.HfX[i][j];
-    const double HfHi = (ix + 1 < TXv) ? S.HfX[i + 1][j] : S.HfXR[iy][j];
-    LineOut lo;
-    line_pass<EXACT, 0>(C, Un, Hn, nLo, nHi, HfLo, HfHi, lo);
-#pragma unroll
-    for (int a = 0; a < NP; ++a) {
-      const int loc = a + NP * j;
-      const double* Uq = Un[a];
-      const Prim<EXACT> q(Uq);
-      const double Hl = Hn[a], Hxl = S.Hx[i][loc], Hyl = S.Hy[i][loc];
-      // source (sgn_flux2d.h:122-134), Manning off
-      const double bath = C.g * (Uq[0] - Hl) + C.gamma * q.p;
-      const double S1 = bath * Hxl, S2 = bath * Hyl, S3 = C.gamma * q.p;
-      const double S4 = C.m2c2 * (q.w + q.u * Hxl + q.v * Hyl);
-      // ncpX (sgn_flux2d.h:150-155)
-      const double Bx = C.mc2 * q.u * lo.dh[a];
-      const double By = S.G[NV][i][loc];
-      const double g0 = S.G[0][i][loc], g1 = S.G[1][i][loc], g2 = S.G[2][i][loc];
-      const double g3 = S.G[3][i][loc], g4 = S.G[4][i][loc];
-      // dU = -dF - dG - Bx - By + S (sgn2d.cpp:285-287); Bx, By vanish except in hp
-      if constexpr (EXACT) {
-        S.G[0][i][loc] = (-lo.d[a][0] - g0) + 0.0;
-        S.G[1][i][loc] = (-lo.d[a][1] - g1) + S1;
-        S.G[2][i][loc] = (-lo.d[a][2] - g2) + S2;
-        S.G[3][i][loc] = (-lo.d[a][3] - g3) + S3;
-        S.G[4][i][loc] = (((-lo.d[a][4] - g4) - Bx) - By) + S4;
-      } else {
-        S.G[0][i][loc] = -(lo.d[a][0] + g0);
-        S.G[1][i][loc] = S1 - (lo.d[a][1] + g1);
-        S.G[2][i][loc] = S2 - (lo.d[a][2] + g2);
-        S.G[3][i][loc] = S3 - (lo.d[a][3] + g3);
-        S.G[4][i][loc] = S4 - (lo.d[a][4] + g4) - Bx - By;
-      }
-    }
+    const double HfLo = hf_x(S, i, j);
+    const double HfHi = (ix + 1 < TXv) ? hf_x(S, i + 1, j) : hf_xr(S, iy, j);
+    double dhx[NP];
+    line_pass<EXACT, 0>(
+        C, Un, Hn, nLo, nHi, HfLo, HfHi,
+        [&](int a, double dh, const Prim<EXACT>&) { dhx[a] = dh; },
+        [&](int a, int v, double d, const Prim<EXACT>& q) {
+          const int loc = a + NP * j;
+          const double g = S.G[v][i][loc];
+          double res;
+          // dU = -dF - dG - Bx - By + S (sgn2d.cpp:285-287) with the source of
+          // sgn_flux2d.h:122-134 (Manning off); Bx, By vanish except in hp
+          if (v == 0) {
+            res = EXACT ? (-d - g) + 0.0 : -(d + g);
+          } else if (v == 3) {
+            const double S3 = C.gamma * q.p;
+            res = EXACT ? (-d - g) + S3 : S3 - (d + g);
+          } else if (v == 1 || v == 2) {
+            const double bath = C.g * (Un[a][0] - Hn[a]) + C.gamma * q.p;
+            const double Sv = bath * (v == 1 ? S.Hx[i][loc] : S.Hy[i][loc]);
+            res = EXACT ? (-d - g) + Sv : Sv - (d + g);
+          } else {
+            const double Hxl = S.Hx[i][loc], Hyl = S.Hy[i][loc];
+            const double S4 = C.m2c2 * (q.w + q.u * Hxl + q.v * Hyl);
+            const double Bx = C.mc2 * q.u * dhx[a];  // ncpX (sgn_flux2d.h:150-155)
+            const double By = S.G[NV][i][loc];
+            res = EXACT ? (((-d - g) - Bx) - By) + S4 : S4 - (d + g) - Bx - By;
+          }
+          S.G[v][i][loc] = res;
+        });
   }
   __syncthreads();
 
   // ---- copy-out (and the embedded error of the FSAL stage) ------------------
   double esum = 0.0, emax = 0.0;
   int enan = 0;
+  item_map();
   {
-    const double* srcU = &S.G[0][0][0];
-    double* outp;
+    // reload the controller values and stage pointers instead of keeping them live
+    // through the passes
+    if constexpr (MODE == MODE_FSAL) {
+      const volatile CtrlState* vc = A.ctrl;
+      cur = vc->cur;
+      I.dt = vc->dt;
+      atol = vc->atol;
+      rtol = vc->rtol;
+      I.u = A.U[cur];
+      I.k1 = A.K1[cur];
+      I.k2 = A.K2;
+      I.k3 = A.K3;
+    }
+    double* __restrict__ outp;
     if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) outp = A.out;
     else outp = A.K1[cur ^ 1];
-    for (int it = tid; it < NV * TY * TX * NPP; it += NTHR) {
-      const int k = it % (TX * NPP);
-      const int r = it / (TX * NPP);
-      const int iy2 = r % TY, v = r / TY;
-      if (iy2 >= TYv || k >= TXv * NPP) continue;
-      const long long eg = (long long)ex0 + (long long)Nx * (ey0 + iy2);
-      const long long gi = (long long)v * Nd + eg * NPP + k;
-      const double val = srcU[(v * TE + iy2 * TX) * NPP + k];
-      outp[gi] = val;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double val[NIT];
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          val[u] = (&S.G[v][0][0])[sof[u]];
+          outp[(long long)v * Nd + gof[u]] = val[u];
+        }
       if constexpr (MODE == MODE_FSAL) {
-        // scaled embedded error, src/solver/rk.cpp:118-128
-        const double u = A.U[cur][gi], k1 = A.K1[cur][gi], k2 = A.K2[gi], k3 = A.K3[gi];
-        const double un = u + dt * (2.0 / 9.0 * k1 + 1.0 / 3.0 * k2 + 4.0 / 9.0 * k3);
-        const double uEmb = u + dt * (7.0 / 24.0 * k1 + 0.25 * k2 + 1.0 / 3.0 * k3 + 0.125 * val);
-        const double e = un - uEmb;
-        const double au = fabs(u), an = fabs(un);
-        const double sc = atol + rtol * (au < an ? an : au);
-        const double rr = e / sc;
-        esum += rr * rr;
-        const double ar = fabs(rr);
-        emax = emax < ar ? ar : emax;
-        enan |= (rr != rr);
+        double uu[NIT], c1[NIT], c2[NIT], c3[NIT];
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            const long long g = (long long)v * Nd + gof[u];
+            uu[u] = I.u[g]; c1[u] = I.k1[g]; c2[u] = I.k2[g]; c3[u] = I.k3[g];
+          }
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            // scaled embedded error, src/solver/rk.cpp:118-128
+            const double dt = I.dt;
+            const double un = uu[u] + dt * (2.0 / 9.0 * c1[u] + 1.0 / 3.0 * c2[u] + 4.0 / 9.0 * c3[u]);
+            const double uEmb = uu[u] + dt * (7.0 / 24.0 * c1[u] + 0.25 * c2[u] + 1.0 / 3.0 * c3[u] +
+                                              0.125 * val[u]);
+            const double e = un - uEmb;
+            const double au = fabs(uu[u]), an = fabs(un);
+            const double sc = atol + rtol * (au < an ? an : au);
+            const double rr = e / sc;
+            esum += rr * rr;
+            const double ar = fabs(rr);
+            emax = emax < ar ? ar : emax;
+            enan |= (rr != rr);
+          }
       }
     }
   }

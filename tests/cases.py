@@ -109,5 +109,5 @@ def cfg2_case(Nx=2048, Ny=1024, Lx=40.0, Ly=20.0, seed=2, chunk=1 << 22):
         for a, l, t, ph in zip(amp, lam, theta, phase):
             k = 2 * np.pi / l
             eta += a * np.sin(k * (xs * np.cos(t) + ys * np.sin(t)) + ph)
-        U[s:s + chunk] = H + eta
+        U[s:s + xs.size] = H + eta
     return kw, U
