@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 hyperbolic-SGN FR right-hand side and BS3(2) stage loop.
+
+Workload: configuration 2 (sgnb.workloads): 2048 x 1024 P=4 elements, 262,144,000 DOF,
+reflective walls, elliptic shoal, 8 random-phase sine waves, FP64. A "step" is one
+accepted adaptive Bogacki-Shampine 3(2) step (3 right-hand-side evaluations per
+attempt, rejected attempts included). Metric: DOF-updates per second per RK stage =
+DOF x RHS evaluations / time (the reference's own throughput definition,
+README.md:369-377 and apps/sgn_bench.cu:138-141 of the reference).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fast|exact]
+    python bench.py --impl reference ...
+
+Our arm prints one JSON line with value (device-resident, CUDA events over K steps,
+max over ranks), e2e (the public API with host buffers: upload from pinned memory,
+K steps, download), roofline of the dominant kernel, clocks, the CPU baseline (the
+oracle port on rank 0) and the number of kernel launches. N > 1 runs independent
+replicas, one per GPU (the path does not exchange data between instances).
+
+The reference arm times the reference's own CPU solver (oracle/_ref, compiled from the
+reference sources; the oracle port when that build is absent) on all host cores as
+independent single-core replicas, each evaluating right-hand sides of a row strip of
+the same configuration-2 mesh, sized so that the run ends within a few minutes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sgn-hyperbolic-gpu_b200"))
+
+METRIC = "DOF-updates/s per RK stage"
+UNIT = "DOF-updates/s"
+# Algorithmic HBM bytes per DOF (8 B doubles): U in and dU out (16), nodal H, Hx, Hy
+# (3 x 8 / 5 fields = 4.8), face depths (2 x 5 per element / 125 DOF x 8 = 0.64).
+STATIC_B = 4.8 + 0.64
+BYTES_PER_DOF = {
+    "rhs": 16.0 + STATIC_B,                  # 21.44
+    "stage": 8 + 8 + STATIC_B + 8,           # u, k in; k_out out: 29.44
+    "fsal": 4 * 8 + STATIC_B + 2 * 8,        # u, k1..k3 in; uNew, k4 out: 53.44
+}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_dof():
+    """DRAM bytes per DOF per kernel mode from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic_per_dof.txt")
+    out = {}
+    try:
+        for line in open(p):
+            line = line.strip()
+            if line and not line.startswith("#") and "=" in line:
+                k, v = line.split("=", 1)
+                out[k.strip()] = float(v)
+    except OSError:
+        pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "out", "") or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import sgnb
+    from sgnb import workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+
+    Nx, Ny, Lx, Ly = W.CFG2["Nx"], W.CFG2["Ny"], W.CFG2["Lx"], W.CFG2["Ly"]
+    kw = W.cfg2_solver_args(Nx, Ny, Lx, Ly)
+    prec = sgnb.FP64_FAST if args.precision == "fast" else sgnb.FP64_EXACT
+    dof = 5 * 25 * Nx * Ny
+    Ud = W.cfg2_state_torch(Nx, Ny, Lx, Ly, device=f"cuda:{local}")
+    U_host = torch.empty(Ud.numel(), dtype=torch.float64, pin_memory=True)
+    U_host.copy_(Ud)
+    del Ud
+    torch.cuda.empty_cache()
+    U_np = U_host.numpy()
+    out_host = torch.empty_like(U_host, pin_memory=True).numpy()
+
+    solver = sgnb.SGN2DB200(precision=prec, device=local, **kw)
+    solver.upload(U_np)
+    dt0 = solver.cfl_time_step(0.5)
+    _, sptr = solver.state_device_ptr()
+    stream = torch.cuda.ExternalStream(sptr, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (graph capture, clocks)
+    solver.integrate_steps(0.0, dt0, max(args.warmup, 1))
+
+    # ---- value: state resident in HBM, CUDA events on the solver's stream ----------
+    solver.upload(U_np)
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        st = solver.integrate_steps(0.0, dt0, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    t_dev = e0.elapsed_time(e1) / 1e3
+    clocks = clk.summary()
+
+    # ---- roofline of the fused stage kernels, timed alone on the same stream -------
+    dt_probe = st.dtLast if st.dtLast > 0 else dt0
+    per = {}
+    for stage, key in ((2, "stage"), (4, "fsal")):
+        solver.launch_stage(stage, dt_probe, 2)
+        torch.cuda.synchronize()
+        reps = 10
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        solver.launch_stage(stage, dt_probe, reps)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        per[key] = a0.elapsed_time(a1) / 1e3 / reps
+    dominant = "fsal" if per["fsal"] >= 2 * per["stage"] else "stage"
+    peak, peak_kind = measured_peak_hbm()
+    achieved = BYTES_PER_DOF[dominant] * dof / per[dominant] / 1e9
+    tpd = traffic_per_dof()
+    traffic = tpd.get(dominant)
+    roofline = {"bound": "hbm", "kernel": f"k_fused ({dominant} mode)",
+                "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": (round(traffic * dof) if traffic else None),
+                "algorithmic_bytes": round(BYTES_PER_DOF[dominant] * dof),
+                "launch_ms": {k: round(v * 1e3, 4) for k, v in per.items()}}
+
+    # ---- e2e through the public API with host buffers ----------------------------
+    torch.cuda.synchronize()
+    barrier()
+    h0 = time.perf_counter()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    solver.upload(U_np)                      # H2D of the step inputs (pinned host)
+    st_e = solver.integrate_steps(0.0, dt0, args.steps)
+    solver.download(out_host)                # D2H of the result (pinned host)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max(e2.elapsed_time(e3) / 1e3, 0.0)
+    t_e2e_host = time.perf_counter() - h0
+    barrier()
+    finite = bool(np.isfinite(out_host[:: max(1, out_host.size // 100000)]).all())
+
+    # ---- gather over ranks (max time, summed work) ------------------------------
+    vals = torch.tensor([t_dev, t_e2e, float(st.rhsEvals), float(st_e.rhsEvals)],
+                        dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        tmax = vals[:2].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        work = vals[2:].clone()
+        dist.all_reduce(work, op=dist.ReduceOp.SUM)
+        t_dev, t_e2e = float(tmax[0]), float(tmax[1])
+        rhs_all, rhs_all_e = float(work[0]), float(work[1])
+    else:
+        rhs_all, rhs_all_e = float(st.rhsEvals), float(st_e.rhsEvals)
+    value = dof * rhs_all / t_dev
+    e2e_value = dof * rhs_all_e / t_e2e
+    state_bytes = 8 * 5 * 25 * Nx * Ny
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(U_np, kw, dof)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "configuration 2: 2048x1024 P=4 (262,144,000 DOF), "
+                                   "40x20 basin with reflective walls, elliptic shoal, "
+                                   "8 random-phase sines; adaptive BS3(2) steps",
+                       "mesh": [Nx, Ny], "dof": dof, "precision": f"fp64-{args.precision}",
+                       "accepted": st.accepted, "rejected": st.rejected,
+                       "rhs_evals": st.rhsEvals, "l2": "inputs larger than L2 "
+                       f"({state_bytes / 1e9:.2f} GB state, 6 state-sized buffers)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": state_bytes / args.steps,
+                    "host_wall_s": t_e2e_host, "final_state_finite": finite},
+            "gpu_launches": int(st.kernel_launches),
+            "roofline": roofline,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline_port(U, kw, dof):
+    """The oracle port (test infrastructure) on 1 host core: two right-hand sides of the
+    full configuration-2 state, walls included."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    o = O.Oracle(**kw)
+    o.rhs(U)
+    n = 1
+    t0 = time.perf_counter()
+    for _ in range(n):
+        o.rhs(U)
+    t = time.perf_counter() - t0
+    return {"value": dof * n / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} rhs evaluation(s) of the full configuration-2 state "
+                      f"(262,144,000 DOF) after one untimed one, {t:.1f} s"}
+
+
+# --------------------------------------------------------------------------- reference arm
+def _ref_worker(args):
+    """One single-core replica: right-hand sides of a row strip of the configuration-2
+    mesh with the reference's CPU solver (its periodic boundary; per-DOF cost is the
+    same), K+W evaluations, the last K timed."""
+    rows, K, Wm, use_ref = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "sgn-hyperbolic-gpu_b200"))
+    import numpy as np
+
+    import oracle as O
+    from sgnb import workloads as W
+
+    kw = W.cfg2_solver_args(2048, rows, 40.0, 20.0 * rows / 1024)
+    kw.update(bc_x=0, bc_y=0)
+    o = O.Oracle(reference=use_ref, **kw)
+    x, y = o.node_coords()
+    shoal, (amp, lam, theta, phase) = W.cfg2_params()
+    dx, dy = (x - shoal[2]) / shoal[4], (y - shoal[3]) / shoal[5]
+    q = np.clip(1.0 - (dx * dx + dy * dy), 0.0, None)
+    h = shoal[0] - (shoal[0] - shoal[1]) * q ** 3
+    for A, L, T, P in zip(amp, lam, theta, phase):
+        h = h + A * np.sin(2 * np.pi / L * (x * np.cos(T) + y * np.sin(T)) + P)
+    z = np.zeros_like(h)
+    U = o.make_state(h, z, z, z, z)
+    for _ in range(Wm):
+        o.rhs(U)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        o.rhs(U)
+    return time.perf_counter() - t0, 5 * o.Nd
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return  # under torchrun the other ranks exit without work
+    import multiprocessing as mp
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    use_ref = O.reference_available()
+    P = os.cpu_count() or 1
+    # size each replica's strip so that K + W evaluations take about two minutes
+    budget_s = 120.0
+    per_eval_s = budget_s / max(args.steps + args.warmup, 1)
+    dof_rate = 2.5e7  # per core, order of magnitude of the reference CPU rhs
+    rows = int(max(2, min(1024 // P, per_eval_s * dof_rate / (2048 * 125))))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(P) as pool:
+        res = pool.map(_ref_worker, [(rows, args.steps, args.warmup, use_ref)] * P)
+    tmax = max(t for t, _ in res)
+    work = sum(d for _, d in res) * args.steps
+    value = work / tmax
+    sample = (f"{P} single-core replicas, each {args.steps} timed rhs evaluations of a "
+              f"2048x{rows} row strip of the configuration-2 mesh "
+              f"({res[0][1]:,} DOF), periodic")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tmax / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "configuration 2 mesh (2048x1024 P=4), reference CPU "
+                               "right-hand side per RK stage", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": P,
+                         "kind": "reference" if use_ref else "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["sgnb", "reference"], default="sgnb")
+    ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -84,12 +84,14 @@ typedef struct {
   double atol, rtol, dtMin, dtMax, safety, facMin, facMax;
 } sgnb_rk_opts;
 
-/* AdaptiveRKStats (src/solver/rk.h:64-72) plus the attempt count and a status. */
+/* AdaptiveRKStats (src/solver/rk.h:64-72) plus the attempt count, a status and the
+ * number of kernels the call launched. */
 typedef struct {
   long long accepted, rejected, rhsEvals, attempts;
   double tReached, dtLast, maxNormLast;
   int aborted;   /* 1: dt < dtMin (as the reference); 2: non-finite error */
   int status;    /* sgnb_status of the run */
+  long long kernel_launches; /* device kernels launched, including no-op tail launches */
 } sgnb_rk_stats;
 
 typedef struct sgnb_ctx sgnb_ctx;
@@ -128,6 +130,12 @@ int sgnb_rhs_device(sgnb_ctx* ctx, const double* U_dev, double* dU_dev, void* st
  * reference returns normally with stats.aborted). */
 int sgnb_integrate_adaptive(sgnb_ctx* ctx, double t0, double tEnd, double dt0,
                             const sgnb_rk_opts* opts, sgnb_rk_stats* stats);
+/* The same device-resident loop run for a fixed number of accepted steps instead of to
+ * an end time (tEnd = infinity, stop after nsteps accepted): the form the benchmark uses
+ * for "N adaptive steps". Built on integrateAdaptive (src/solver/rk.h:78-80); the
+ * reference has no step-count stop. */
+int sgnb_integrate_steps(sgnb_ctx* ctx, double t0, double dt0, long long nsteps,
+                         const sgnb_rk_opts* opts, sgnb_rk_stats* stats);
 /* n consecutive bs3Step (src/solver/rk.h:50) steps of the uploaded state with the
  * given step sizes, starting at t0: the frozen-dt replay of an accepted sequence. */
 int sgnb_bs3_steps(sgnb_ctx* ctx, double t0, const double* dts, long long n);
@@ -137,6 +145,14 @@ int sgnb_bs3_steps(sgnb_ctx* ctx, double t0, const double* dts, long long n);
  * rows into out and sets *n to the number recorded. No reference counterpart (the
  * reference keeps only AdaptiveRKStats); it exposes the controller's dt sequence. */
 int sgnb_attempt_log(sgnb_ctx* ctx, double* out, long long cap, long long* n);
+
+/* Profiling hook, no reference counterpart: launches `count` copies of one fused stage
+ * kernel of a BS3(2) attempt (stage 2: k2 = R(u + dt/2 k1); 3: k3 = R(u + 3dt/4 k2);
+ * 4: the end-point stage with uNew, k4 and the error partials) on the uploaded state with
+ * step dt, on `stream` (NULL = context stream), asynchronously. It overwrites only the
+ * stage buffers, so the uploaded state is unchanged; run an integration first so that
+ * k1 is defined. */
+int sgnb_launch_stage(sgnb_ctx* ctx, int stage, double dt, int count, void* stream);
 
 /* SGN2D::maxWaveSpeed / cflTimeStep / mass / energy (src/solver/sgn2d.h:85-90) of the
  * uploaded state, reduced on the device. */

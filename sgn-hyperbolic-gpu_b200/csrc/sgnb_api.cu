@@ -46,6 +46,8 @@ struct sgnb_ctx {
   cudaGraphExec_t chunk = nullptr;
   int chunkLen = 0;
   cudaEvent_t evRead = nullptr;
+  long long launches = 0;  // kernels launched by the last integration
+  long long pendingMaxAccepted = 0;  // set by sgnb_integrate_steps
   int cur = 0;
   std::string err;
 };
@@ -200,9 +202,11 @@ int build_chunk_graph(sgnb_ctx* c, int len) {
 
 // Drive the device-resident loop until the controller reports done.
 int run_loop(sgnb_ctx* c) {
-  int rc = build_chunk_graph(c, 16);
+  const int len = 16;
+  int rc = build_chunk_graph(c, len);
   if (rc) return rc;
   SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
+  c->launches = 1 + 4LL * len;  // head + the first chunk
   // FSAL head: k1 = R(u)
   {
     StageArgs A = base_args(c);
@@ -216,6 +220,7 @@ int run_loop(sgnb_ctx* c) {
   SGNB_CU(c, cudaEventRecord(c->evRead, c->stream));
   for (long long guard = 0;; ++guard) {
     SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
+    c->launches += 4LL * len;
     SGNB_CU(c, cudaEventSynchronize(c->evRead));
     if (c->hctrl->done) break;
     SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
@@ -463,6 +468,7 @@ int sgnb_integrate_adaptive(sgnb_ctx* c, double t0, double tEnd, double dt0,
   h.tReached = t0;
   h.cur = c->cur;
   h.rhsEvals = 1;  // FSAL head
+  h.maxAccepted = c->pendingMaxAccepted;
   // loop test and end-time clip of the first attempt (rk.cpp:95-97)
   if (!(h.t < tEnd - 1e-15 * ((1.0 < std::fabs(tEnd)) ? std::fabs(tEnd) : 1.0))) h.done = 1;
   else if (h.t + h.dt > tEnd) h.dt = tEnd - h.t;
@@ -474,8 +480,48 @@ int sgnb_integrate_adaptive(sgnb_ctx* c, double t0, double tEnd, double dt0,
     st->maxNormLast = h.maxNormLast;
     st->aborted = h.done == 2 ? 1 : (h.done == 3 ? 2 : 0);
     st->status = h.done == 3 ? SGNB_ERR_NAN : SGNB_OK;
+    st->kernel_launches = c->launches;
   }
   if (h.done == 3) return fail(c, SGNB_ERR_NAN, "non-finite embedded error estimate");
+  return SGNB_OK;
+}
+
+int sgnb_integrate_steps(sgnb_ctx* c, double t0, double dt0, long long nsteps,
+                         const sgnb_rk_opts* opts, sgnb_rk_stats* st) {
+  if (!c || nsteps < 1) return fail(c, SGNB_ERR_INVALID, "nsteps must be >= 1");
+  c->hctrl->maxAccepted = 0;
+  c->pendingMaxAccepted = nsteps;
+  const int rc = sgnb_integrate_adaptive(c, t0, 1e300, dt0, opts, st);
+  c->pendingMaxAccepted = 0;
+  return rc;
+}
+
+int sgnb_launch_stage(sgnb_ctx* c, int stage, double dt, int count, void* stream) {
+  if (!c || stage < 2 || stage > 4 || count < 1 || !(dt > 0))
+    return fail(c, SGNB_ERR_INVALID, "stage in 2..4, count >= 1, dt > 0");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  CtrlState& h = *c->hctrl;
+  sgnb_rk_opts o;
+  sgnb_rk_opts_init(&o);
+  init_ctrl(c, h, o);
+  h.t = 0.0;
+  h.tEnd = 1e300;
+  h.dt = dt;
+  h.cur = c->cur;
+  h.log = nullptr;
+  SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < count; ++k) {
+    StageArgs A = base_args(c);
+    if (stage == 4) {
+      SGNB_CU(c, launch(c, 2, A, s));
+    } else {
+      A.kin_k2 = stage == 3 ? 1 : 0;
+      A.coef = stage == 3 ? 0.75 : 0.5;
+      A.out = stage == 3 ? c->K3 : c->K2;
+      SGNB_CU(c, launch(c, 1, A, s));
+    }
+  }
   return SGNB_OK;
 }
 

@@ -47,6 +47,7 @@ struct CtrlState {
   long long nList;
   double* log;           // attempt log: (t, dt, errNorm, accepted) per attempt
   long long logCap;      // capacity of the log in attempts
+  long long maxAccepted; // > 0: stop after this many accepted steps
 };
 
 // Buffers of one fused launch.

@@ -70,6 +70,7 @@ __global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const
     c->dt = c->dtList[c->accepted];
     return;
   }
+  bool stop = false;
   if (errNorm <= 1.0) {
     c->t += c->dt;
     c->cur ^= 1;  // uNew becomes u and k4 becomes k1 (FSAL)
@@ -78,6 +79,7 @@ __global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const
     c->dtLast = c->dt;
     c->maxNormLast = errMax;
     c->errPrev = errNorm;
+    stop = c->maxAccepted > 0 && c->accepted >= c->maxAccepted;
   } else {
     c->rejected += 1;
   }
@@ -92,6 +94,7 @@ __global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const
     return;
   }
   c->dt = dtNext;
+  if (stop) { c->done = 1; return; }  // fixed number of accepted steps reached
   const double tEnd = c->tEnd;
   if (!(c->t < tEnd - 1e-15 * dmax(1.0, fabs(tEnd)))) { c->done = 1; return; }
   if (c->t + c->dt > tEnd) c->dt = tEnd - c->t;

@@ -77,7 +77,7 @@ class _Stats(C.Structure):
     _fields_ = [("accepted", C.c_longlong), ("rejected", C.c_longlong),
                 ("rhsEvals", C.c_longlong), ("attempts", C.c_longlong),
                 ("tReached", C.c_double), ("dtLast", C.c_double), ("maxNormLast", C.c_double),
-                ("aborted", C.c_int), ("status", C.c_int)]
+                ("aborted", C.c_int), ("status", C.c_int), ("kernel_launches", C.c_longlong)]
 
 
 @dataclasses.dataclass
@@ -103,6 +103,7 @@ class AdaptiveRKStats:
     dtLast: float = 0.0
     maxNormLast: float = 0.0
     aborted: int = 0
+    kernel_launches: int = 0
 
 
 _lib = None
@@ -121,7 +122,10 @@ SIGNATURES = {
     "sgnb_rhs_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sgnb_integrate_adaptive": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
                                           C.POINTER(_Opts), C.POINTER(_Stats)]),
+    "sgnb_integrate_steps": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_longlong,
+                                       C.POINTER(_Opts), C.POINTER(_Stats)]),
     "sgnb_bs3_steps": (C.c_int, [C.c_void_p, C.c_double, _dp, C.c_longlong]),
+    "sgnb_launch_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_void_p]),
     "sgnb_attempt_log": (C.c_int, [C.c_void_p, _dp, C.c_longlong, C.POINTER(C.c_longlong)]),
     "sgnb_max_wave_speed": (C.c_int, [C.c_void_p, _dp]),
     "sgnb_cfl_time_step": (C.c_int, [C.c_void_p, C.c_double, _dp]),
@@ -338,7 +342,24 @@ class SGN2DB200:
         if rc != 0 and (raise_on_nan or rc != 4):
             _check(rc, self._h)
         return AdaptiveRKStats(st.accepted, st.rejected, st.rhsEvals, st.attempts,
-                               st.tReached, st.dtLast, st.maxNormLast, st.aborted)
+                               st.tReached, st.dtLast, st.maxNormLast, st.aborted,
+                               st.kernel_launches)
+
+    def integrate_steps(self, t0, dt0, nsteps, opt: AdaptiveRKOptions | None = None
+                        ) -> AdaptiveRKStats:
+        """The device-resident loop for a fixed number of accepted steps."""
+        o = _Opts(**dataclasses.asdict(opt or AdaptiveRKOptions()))
+        st = _Stats()
+        _check(lib().sgnb_integrate_steps(self._h, t0, dt0, int(nsteps), C.byref(o),
+                                          C.byref(st)), self._h)
+        return AdaptiveRKStats(st.accepted, st.rejected, st.rhsEvals, st.attempts,
+                               st.tReached, st.dtLast, st.maxNormLast, st.aborted,
+                               st.kernel_launches)
+
+    def launch_stage(self, stage: int, dt: float, count: int = 1, stream: int | None = None):
+        """Profiling hook: `count` launches of one fused stage kernel (2, 3 or 4)."""
+        s = None if stream is None else C.c_void_p(stream if stream else _CUDA_STREAM_LEGACY)
+        _check(lib().sgnb_launch_stage(self._h, stage, dt, count, s), self._h)
 
     def bs3_steps(self, t0, dts):
         """Consecutive bs3Step calls with the given step sizes (frozen-dt replay)."""

@@ -1,0 +1,67 @@
+"""Workload definitions: the benchmark configurations as solver arguments plus a state.
+
+Configuration 2 (the benchmark workload): 2048 x 1024 elements, P = 4, on a 40 x 20 basin
+with reflective walls. Still depth: a 0.45 plane with an elliptic shoal centred at
+(20, 10), semi-axes 4 (x) and 3 (y), crest depth 0.15, profile
+H = 0.45 - 0.30 (1 - r^2)^3 inside the ellipse. Free surface: the sum of 8 sine waves with
+seeded random phase, direction, amplitude in [0.005, 0.02] and wavelength in [1, 4]
+(numpy default_rng(2)); zero initial velocity, w = p = 0. alpha = 3 with c = alpha sqrt(g H0),
+H0 = 0.45; gamma = 1.5. 500 adaptive BS3(2) steps, atol 1e-8, rtol 1e-6.
+
+States are built in float64 with torch on the device (fast at 52M nodes) or with numpy on
+the host; the two agree to libm rounding, and each run feeds one state to every solver it
+compares.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+G, GAMMA, ALPHA = 9.81, 1.5, 3.0
+CFG2 = dict(Nx=2048, Ny=1024, Lx=40.0, Ly=20.0, steps=500)
+
+
+def cfg2_params(seed: int = 2):
+    """Depth profile (BATHY_SHOAL parameters) and the 8 wave components."""
+    shoal = (0.45, 0.15, 20.0, 10.0, 4.0, 3.0)
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.005, 0.02, 8)
+    lam = rng.uniform(1.0, 4.0, 8)
+    theta = rng.uniform(0.0, 2 * np.pi, 8)
+    phase = rng.uniform(0.0, 2 * np.pi, 8)
+    return shoal, (amp, lam, theta, phase)
+
+
+def cfg2_solver_args(Nx=2048, Ny=1024, Lx=40.0, Ly=20.0, seed=2):
+    shoal, _ = cfg2_params(seed)
+    return dict(P=4, Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, g=G, c=ALPHA * math.sqrt(G * shoal[0]),
+                gamma=GAMMA, bc_x=1, bc_y=1, bathy_kind=3, bathy_par=shoal)
+
+
+def cfg2_state_torch(Nx=2048, Ny=1024, Lx=40.0, Ly=20.0, seed=2, device="cuda"):
+    """Initial state of configuration 2 as a float64 torch tensor (var-major layout)."""
+    import torch
+
+    shoal, (amp, lam, theta, phase) = cfg2_params(seed)
+    s = math.sqrt(3.0 / 7.0)
+    nodes = torch.tensor([-1.0, -s, 0.0, s, 1.0], dtype=torch.float64, device=device)
+    hx, hy = Lx / Nx, Ly / Ny
+    a = torch.arange(5, device=device).repeat(5)
+    b = torch.arange(5, device=device).repeat_interleave(5)
+    U = torch.zeros(5, Ny, Nx, 25, dtype=torch.float64, device=device)
+    ex = torch.arange(Nx, device=device, dtype=torch.float64)
+    for r0 in range(0, Ny, 64):  # bounded temporaries
+        ey = torch.arange(r0, min(r0 + 64, Ny), device=device, dtype=torch.float64)
+        x = (ex[None, :, None] * hx + 0.5 * hx * (nodes[a][None, None, :] + 1.0))
+        y = (ey[:, None, None] * hy + 0.5 * hy * (nodes[b][None, None, :] + 1.0))
+        x, y = torch.broadcast_tensors(x, y)
+        dx, dy = (x - shoal[2]) / shoal[4], (y - shoal[3]) / shoal[5]
+        q = torch.clamp(1.0 - (dx * dx + dy * dy), min=0.0)
+        H = shoal[0] - (shoal[0] - shoal[1]) * q ** 3
+        eta = torch.zeros_like(x)
+        for A, L, T, P in zip(amp, lam, theta, phase):
+            k = 2 * math.pi / L
+            eta += A * torch.sin(k * (x * math.cos(T) + y * math.sin(T)) + P)
+        U[0, r0:r0 + ey.numel()] = H + eta
+    return U.reshape(-1)
