@@ -161,6 +161,23 @@ int sgnb_cfl_time_step(sgnb_ctx* ctx, double cfl, double* out);
 int sgnb_mass(sgnb_ctx* ctx, double* out);
 int sgnb_energy(sgnb_ctx* ctx, double* out);
 
+/* Allocation-free variant of sgnb_max_wave_speed / sgnb_mass / sgnb_energy, without a
+ * context; no counterpart in the reference. For callers that cannot allocate device
+ * memory (a framework that owns all of it through its own pool, or a fixed-budget loop
+ * that must not call cudaMalloc between steps): it allocates nothing and keeps its
+ * per-block partials in a library-owned 128 KB __device__ array instead.
+ * what = 0 largest wave speed, 1 mass, 2 energy of the state U_dev (device, the layout
+ * above, 25 Nx Ny nodes per field); Hnod_dev (device, nodal still depth) is read only
+ * for the energy. The result is written to out_dev[0] (device) asynchronously on
+ * `stream` (NULL = the legacy default stream) on the current device.
+ * Limit: 25 Nx Ny <= 67,108,864 nodes per field, else SGNB_ERR_INVALID.
+ * The first call on a device looks up the array's device address; make that first call
+ * before any stream capture. All calls on a device share the array: calls that overlap
+ * on the GPU race. */
+int sgnb_diag_noalloc(int what, int Nx, int Ny, double Lx, double Ly, double g, double c,
+                      double gamma, const double* U_dev, const double* Hnod_dev,
+                      double* out_dev, void* stream);
+
 /* Host-side set-up queries (no device work). */
 /* SGN2D::nodeCoords (src/solver/sgn2d.h:70). */
 int sgnb_node_coords(const sgnb_ctx* ctx, double* x, double* y);

@@ -131,6 +131,9 @@ SIGNATURES = {
     "sgnb_cfl_time_step": (C.c_int, [C.c_void_p, C.c_double, _dp]),
     "sgnb_mass": (C.c_int, [C.c_void_p, _dp]),
     "sgnb_energy": (C.c_int, [C.c_void_p, _dp]),
+    "sgnb_diag_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]),
     "sgnb_node_coords": (C.c_int, [C.c_void_p, _dp, _dp]),
     "sgnb_state_device_ptr": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p)]),
