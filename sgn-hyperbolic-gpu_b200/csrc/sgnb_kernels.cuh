@@ -630,31 +630,44 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
     double* __restrict__ outp;
     if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) outp = A.out;
     else outp = A.K1[cur ^ 1];
+    if constexpr (MODE != MODE_FSAL) {
+#pragma unroll 1
+      for (int v = 0; v < NV; ++v)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      double val[NIT];
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) outp[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
+    } else {
+      // One field at a time, with the next field's four arrays prefetched while the
+      // current field's error is formed: hoisting every field's loads at once would
+      // overflow the register budget.
+      double uu[NIT], c1[NIT], c2[NIT], c3[NIT];
+      double nu[NIT], n1[NIT], n2[NIT], n3[NIT];
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
-          val[u] = (&S.G[v][0][0])[sof[u]];
-          outp[(long long)v * Nd + gof[u]] = val[u];
+          const long long g = gof[u];
+          uu[u] = I.u[g]; c1[u] = I.k1[g]; c2[u] = I.k2[g]; c3[u] = I.k3[g];
         }
-      if constexpr (MODE == MODE_FSAL) {
-        double uu[NIT], c1[NIT], c2[NIT], c3[NIT];
+#pragma unroll 1
+      for (int v = 0; v < NV; ++v) {
+        if (v + 1 < NV) {
+#pragma unroll
+          for (int u = 0; u < NIT; ++u)
+            if (okk[u]) {
+              const long long g = (long long)(v + 1) * Nd + gof[u];
+              nu[u] = I.u[g]; n1[u] = I.k1[g]; n2[u] = I.k2[g]; n3[u] = I.k3[g];
+            }
+        }
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
-            const long long g = (long long)v * Nd + gof[u];
-            uu[u] = I.u[g]; c1[u] = I.k1[g]; c2[u] = I.k2[g]; c3[u] = I.k3[g];
-          }
-#pragma unroll
-        for (int u = 0; u < NIT; ++u)
-          if (okk[u]) {
+            const double k4 = (&S.G[v][0][0])[sof[u]];
+            outp[(long long)v * Nd + gof[u]] = k4;
             // scaled embedded error, src/solver/rk.cpp:118-128
             const double dt = I.dt;
             const double un = uu[u] + dt * (2.0 / 9.0 * c1[u] + 1.0 / 3.0 * c2[u] + 4.0 / 9.0 * c3[u]);
             const double uEmb = uu[u] + dt * (7.0 / 24.0 * c1[u] + 0.25 * c2[u] + 1.0 / 3.0 * c3[u] +
-                                              0.125 * val[u]);
+                                              0.125 * k4);
             const double e = un - uEmb;
             const double au = fabs(uu[u]), an = fabs(un);
             const double sc = atol + rtol * (au < an ? an : au);
@@ -664,6 +677,10 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
             emax = emax < ar ? ar : emax;
             enan |= (rr != rr);
           }
+#pragma unroll
+        for (int u = 0; u < NIT; ++u) {
+          uu[u] = nu[u]; c1[u] = n1[u]; c2[u] = n2[u]; c3[u] = n3[u];
+        }
       }
     }
   }
