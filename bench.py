@@ -123,6 +123,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def reduce_over_ranks(times, works, dist, device):
+    """Replica aggregation: the slowest rank's times (max) and the summed work of all
+    ranks. Every rank takes the same two collective steps; dist None = one process."""
+    if dist is None:
+        return list(times), list(works)
+    import torch
+
+    t = torch.tensor(times, dtype=torch.float64, device=device)
+    w = torch.tensor(works, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return t.tolist(), w.tolist()
+
+
 # --------------------------------------------------------------------------- our arm
 def run_ours(args):
     import numpy as np
@@ -227,17 +241,8 @@ def run_ours(args):
     finite = bool(np.isfinite(out_host[:: max(1, out_host.size // 100000)]).all())
 
     # ---- gather over ranks (max time, summed work) ------------------------------
-    vals = torch.tensor([t_dev, t_e2e, float(st.rhsEvals), float(st_e.rhsEvals)],
-                        dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        tmax = vals[:2].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        work = vals[2:].clone()
-        dist.all_reduce(work, op=dist.ReduceOp.SUM)
-        t_dev, t_e2e = float(tmax[0]), float(tmax[1])
-        rhs_all, rhs_all_e = float(work[0]), float(work[1])
-    else:
-        rhs_all, rhs_all_e = float(st.rhsEvals), float(st_e.rhsEvals)
+    (t_dev, t_e2e), (rhs_all, rhs_all_e) = reduce_over_ranks(
+        [t_dev, t_e2e], [float(st.rhsEvals), float(st_e.rhsEvals)], dist, f"cuda:{local}")
     value = dof * rhs_all / t_dev
     e2e_value = dof * rhs_all_e / t_e2e
     state_bytes = 8 * 5 * 25 * Nx * Ny
