@@ -38,10 +38,13 @@ typedef enum {
 
 enum { SGNB_BC_PERIODIC = 0, SGNB_BC_WALL = 1 };
 
-/* Arithmetic modes of the FP64 path. */
+/* Arithmetic modes. */
 enum {
   SGNB_FP64_EXACT = 0, /* reference operation order, no FMA: bit-identical to the CPU */
-  SGNB_FP64_FAST = 1   /* FMA + reciprocals: within 1e-13 relative per field */
+  SGNB_FP64_FAST = 1,  /* FMA + reciprocals: within 1e-13 relative per field */
+  SGNB_MIXED = 2       /* FP32 deviations from the lake at rest, FP64 hydrostatic balance,
+                          FP64 state / RK accumulation / error / controller, FP32 stage
+                          derivatives (an addition to the reference, which is FP64 only) */
 };
 
 /* Built-in still-depth profiles H(x, y); SGNB_BATHY_ARRAYS takes precomputed arrays.
@@ -66,7 +69,7 @@ typedef struct {
   double Lx, Ly;
   double g, c, gamma, nManning; /* nManning must be 0 (Manning friction is not built) */
   int bc_x, bc_y;            /* SGNB_BC_*; walls are an addition to the reference */
-  int precision;             /* SGNB_FP64_* */
+  int precision;             /* SGNB_FP64_EXACT, SGNB_FP64_FAST or SGNB_MIXED */
   int device;                /* CUDA device ordinal */
   /* FR tables of FROperators1D (src/core/fr_operators.h:68-89); all NULL = built here */
   const double *nodes, *D, *lL, *lR, *gLp, *gRp, *qw;

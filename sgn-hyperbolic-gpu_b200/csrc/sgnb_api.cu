@@ -30,9 +30,11 @@ struct sgnb_ctx {
   RhsConsts C{};
   double* Hbuf = nullptr;  // one allocation holding all statics
   double* U[2] = {nullptr, nullptr};
-  double* K1[2] = {nullptr, nullptr};
-  double* K2 = nullptr;
-  double* K3 = nullptr;
+  // stage derivatives: FP64 (exact / fast) or FP32 (mixed precision)
+  void* K1[2] = {nullptr, nullptr};
+  void* K2 = nullptr;
+  void* K3 = nullptr;
+  bool mixed = false;
   double* partials = nullptr;
   int nblk = 0;
   double* diag = nullptr;  // diagnostic partials
@@ -72,19 +74,54 @@ int cuda_fail(sgnb_ctx* c, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
-cudaError_t launch(sgnb_ctx* c, int mode, const StageArgs& A, cudaStream_t s) {
-  return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(mode, c->C, A, s)
-                                        : dev::launch_fused_exact(mode, c->C, A, s);
-}
+// One fused launch: mode 0 rhs (in -> out), 1 stage (u + coef dt k -> K2 or K3),
+// 2 end-point stage. Dispatches on the arithmetic mode of the context.
+struct Launch {
+  int mode = 0;
+  const double* in = nullptr;  // mode 0
+  double* out = nullptr;       // mode 0
+  int stage = 2;               // mode 1: 2 (k1 -> K2) or 3 (k2 -> K3)
+};
 
-StageArgs base_args(sgnb_ctx* c) {
+cudaError_t launch(sgnb_ctx* c, const Launch& L, cudaStream_t s) {
+  if (c->mixed) {
+    StageArgsM A{};
+    A.U[0] = c->U[0]; A.U[1] = c->U[1];
+    A.K1[0] = (float*)c->K1[0]; A.K1[1] = (float*)c->K1[1];
+    A.K2 = (float*)c->K2; A.K3 = (float*)c->K3;
+    A.ctrl = c->dctrl;
+    A.partials = c->partials;
+    A.in = L.in;
+    A.outd = L.out;
+    A.kin_k2 = L.stage == 3;
+    A.coef = L.stage == 3 ? 0.75 : 0.5;
+    if (L.mode == 0) A.out = L.out ? nullptr : A.K1[c->cur];  // no FP64 output: the FSAL head
+    else A.out = L.stage == 3 ? A.K3 : A.K2;
+    return dev::launch_fused_mixed(L.mode, c->C, A, s);
+  }
   StageArgs A{};
   A.U[0] = c->U[0]; A.U[1] = c->U[1];
-  A.K1[0] = c->K1[0]; A.K1[1] = c->K1[1];
-  A.K2 = c->K2; A.K3 = c->K3;
+  A.K1[0] = (double*)c->K1[0]; A.K1[1] = (double*)c->K1[1];
+  A.K2 = (double*)c->K2; A.K3 = (double*)c->K3;
   A.ctrl = c->dctrl;
   A.partials = c->partials;
-  return A;
+  A.in = L.in;
+  A.kin_k2 = L.stage == 3;
+  A.coef = L.stage == 3 ? 0.75 : 0.5;
+  A.out = L.mode == 0 ? L.out : (L.stage == 3 ? A.K3 : A.K2);
+  return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(L.mode, c->C, A, s)
+                                        : dev::launch_fused_exact(L.mode, c->C, A, s);
+}
+
+Launch rhs_launch(const double* in, double* out) {
+  Launch L;
+  L.mode = 0; L.in = in; L.out = out;
+  return L;
+}
+Launch stage_launch(int stage) {
+  Launch L;
+  if (stage == 4) { L.mode = 2; } else { L.mode = 1; L.stage = stage; }
+  return L;
 }
 
 int set_device(sgnb_ctx* c) {
@@ -101,7 +138,8 @@ int check_desc(const sgnb_desc* d) {
     return fail(nullptr, SGNB_ERR_UNSUPPORTED, "Manning friction is not built");
   if (d->bc_x < 0 || d->bc_x > 1 || d->bc_y < 0 || d->bc_y > 1)
     return fail(nullptr, SGNB_ERR_INVALID, "bc must be SGNB_BC_PERIODIC or SGNB_BC_WALL");
-  if (d->precision != SGNB_FP64_EXACT && d->precision != SGNB_FP64_FAST)
+  if (d->precision != SGNB_FP64_EXACT && d->precision != SGNB_FP64_FAST &&
+      d->precision != SGNB_MIXED)
     return fail(nullptr, SGNB_ERR_UNSUPPORTED, "unknown precision mode");
   if ((long long)d->Nx * d->Ny > (1ll << 31) / 25)
     return fail(nullptr, SGNB_ERR_INVALID, "mesh too large");
@@ -178,15 +216,11 @@ int build_chunk_graph(sgnb_ctx* c, int len) {
   SGNB_CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < len && e == cudaSuccess; ++k) {
-    StageArgs A = base_args(c);
-    A.kin_k2 = 0; A.coef = 0.5; A.out = c->K2;  // k2 = R(u + dt/2 k1)
-    e = launch(c, 1, A, c->stream);
+    e = launch(c, stage_launch(2), c->stream);  // k2 = R(u + dt/2 k1)
     if (e != cudaSuccess) break;
-    A.kin_k2 = 1; A.coef = 0.75; A.out = c->K3;  // k3 = R(u + 3dt/4 k2)
-    e = launch(c, 1, A, c->stream);
+    e = launch(c, stage_launch(3), c->stream);  // k3 = R(u + 3dt/4 k2)
     if (e != cudaSuccess) break;
-    StageArgs F = base_args(c);
-    e = launch(c, 2, F, c->stream);  // uNew, k4 = R(uNew), error partials
+    e = launch(c, stage_launch(4), c->stream);  // uNew, k4 = R(uNew), error partials
     if (e != cudaSuccess) break;
     e = dev::launch_controller(c->dctrl, c->partials, c->nblk, c->ntot, c->stream);
   }
@@ -208,12 +242,9 @@ int run_loop(sgnb_ctx* c) {
   SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
   c->launches = 1 + 4LL * len;  // head + the first chunk
   // FSAL head: k1 = R(u)
-  {
-    StageArgs A = base_args(c);
-    A.in = c->U[c->cur];
-    A.out = c->K1[c->cur];
-    SGNB_CU(c, launch(c, 0, A, c->stream));
-  }
+  // FSAL head: k1 = R(u) into K1[cur] (FP32 in the mixed mode)
+  SGNB_CU(c, launch(c, rhs_launch(c->U[c->cur], c->mixed ? nullptr : (double*)c->K1[c->cur]),
+                    c->stream));
   // two chunks in flight: enqueue chunk k+1 before waiting for chunk k's readback
   SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
   SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
@@ -318,6 +349,7 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   c->desc.HfaceXEnd = c->desc.HfaceYEnd = nullptr;
   c->device = d->device;
   c->precision = d->precision;
+  c->mixed = d->precision == SGNB_MIXED;
   if ((rc = tables_for(d, c->tab))) { delete c; return rc; }
   c->mesh = mesh_for(d);
   const long long ne = (long long)d->Nx * d->Ny;
@@ -327,6 +359,7 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   if ((rc = set_device(c))) { g_create_error = c->err; delete c; return rc; }
   e = dev::prepare_fused_exact();
   if (e == cudaSuccess) e = dev::prepare_fused_fast();
+  if (e == cudaSuccess) e = dev::prepare_fused_mixed();
   if (e != cudaSuccess) { cuda_fail(c, e, "kernel attributes"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
 
   // statics: Hnod, Hx, Hy (Nd each), HfX, HfY (5 ne each), HfXEnd (5 Ny), HfYEnd (5 Nx)
@@ -365,11 +398,20 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   fill_consts(c);
 
   const size_t sbytes = (size_t)c->ntot * sizeof(double);
-  double** bufs[6] = {&c->U[0], &c->U[1], &c->K1[0], &c->K1[1], &c->K2, &c->K3};
-  for (auto* bp : bufs) {
+  // stage derivatives are FP32 in the mixed mode; K2 and K3 are allocated as one block so
+  // that together they always hold an FP64 state (scratch for sgnb_rhs_host)
+  const size_t kbytes = (size_t)c->ntot * (c->mixed ? sizeof(float) : sizeof(double));
+  for (double** bp : {&c->U[0], &c->U[1]}) {
     e = cudaMalloc(bp, sbytes);
     if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(state)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
   }
+  for (void** bp : {&c->K1[0], &c->K1[1]}) {
+    e = cudaMalloc(bp, kbytes);
+    if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(stage)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
+  }
+  e = cudaMalloc(&c->K2, 2 * kbytes);
+  if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(stage)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
+  c->K3 = (char*)c->K2 + kbytes;
   e = cudaMemset(c->U[0], 0, sbytes);
   c->nblk = dev::fused_grid_blocks(d->Nx, d->Ny);
   c->ndiag = 592;
@@ -396,7 +438,7 @@ int sgnb_destroy(sgnb_ctx* c) {
   if (c->evRead) cudaEventDestroy(c->evRead);
   cudaFree(c->Hbuf);
   for (int k = 0; k < 2; ++k) { cudaFree(c->U[k]); cudaFree(c->K1[k]); }
-  cudaFree(c->K2); cudaFree(c->K3);
+  cudaFree(c->K2);  // K3 lives in the same block
   cudaFree(c->partials); cudaFree(c->diag); cudaFree(c->dctrl); cudaFree(c->dtList);
   cudaFree(c->alog);
   if (c->hctrl) cudaFreeHost(c->hctrl);
@@ -426,19 +468,16 @@ int sgnb_download(sgnb_ctx* c, double* U) {
 int sgnb_rhs_device(sgnb_ctx* c, const double* Ud, double* dUd, void* stream) {
   if (!c || !Ud || !dUd) return fail(c, SGNB_ERR_INVALID, "NULL argument");
   if (Ud == dUd) return fail(c, SGNB_ERR_INVALID, "input and output must not alias");
-  StageArgs A = base_args(c);
-  A.in = Ud;
-  A.out = dUd;
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-  SGNB_CU(c, launch(c, 0, A, s));
+  SGNB_CU(c, launch(c, rhs_launch(Ud, dUd), s));
   return SGNB_OK;
 }
 
 int sgnb_rhs_once(sgnb_ctx* c, double* dU) {
   if (!c || !dU) return fail(c, SGNB_ERR_INVALID, "NULL argument");
   if (int rc = set_device(c)) return rc;
-  if (int rc = sgnb_rhs_device(c, c->U[c->cur], c->K2, c->stream)) return rc;
-  SGNB_CU(c, cudaMemcpyAsync(dU, c->K2, c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (int rc = sgnb_rhs_device(c, c->U[c->cur], c->U[c->cur ^ 1], c->stream)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(dU, c->U[c->cur ^ 1], c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SGNB_CU(c, cudaStreamSynchronize(c->stream));
   return SGNB_OK;
 }
@@ -446,9 +485,14 @@ int sgnb_rhs_once(sgnb_ctx* c, double* dU) {
 int sgnb_rhs_host(sgnb_ctx* c, const double* U, double* dU) {
   if (!c || !U || !dU) return fail(c, SGNB_ERR_INVALID, "NULL argument");
   if (int rc = set_device(c)) return rc;
-  SGNB_CU(c, cudaMemcpyAsync(c->K3, U, c->ntot * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  if (int rc = sgnb_rhs_device(c, c->K3, c->K2, c->stream)) return rc;
-  SGNB_CU(c, cudaMemcpyAsync(dU, c->K2, c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  // scratch: the spare state buffer holds the input; the output goes over it in place
+  // is not allowed, so the input goes to U[cur ^ 1] and the output to the FP64 view of the
+  // stage buffers (K2, K3 together hold one FP64 state in every precision mode)
+  double* in = c->U[c->cur ^ 1];
+  double* out = c->mixed ? (double*)c->K2 : (double*)c->K3;
+  SGNB_CU(c, cudaMemcpyAsync(in, U, c->ntot * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (int rc = sgnb_rhs_device(c, in, out, c->stream)) return rc;
+  SGNB_CU(c, cudaMemcpyAsync(dU, out, c->ntot * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   SGNB_CU(c, cudaStreamSynchronize(c->stream));
   return SGNB_OK;
 }
@@ -511,17 +555,7 @@ int sgnb_launch_stage(sgnb_ctx* c, int stage, double dt, int count, void* stream
   h.cur = c->cur;
   h.log = nullptr;
   SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, s));
-  for (int k = 0; k < count; ++k) {
-    StageArgs A = base_args(c);
-    if (stage == 4) {
-      SGNB_CU(c, launch(c, 2, A, s));
-    } else {
-      A.kin_k2 = stage == 3 ? 1 : 0;
-      A.coef = stage == 3 ? 0.75 : 0.5;
-      A.out = stage == 3 ? c->K3 : c->K2;
-      SGNB_CU(c, launch(c, 1, A, s));
-    }
-  }
+  for (int k = 0; k < count; ++k) SGNB_CU(c, launch(c, stage_launch(stage), s));
   return SGNB_OK;
 }
 

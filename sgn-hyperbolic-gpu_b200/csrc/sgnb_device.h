@@ -64,6 +64,21 @@ struct StageArgs {
   double* partials;   // MODE_FSAL: 3 doubles per CTA (sum r^2, max |r|, NaN count)
 };
 
+// Buffers of one mixed-precision launch: FP64 state, FP32 stage derivatives.
+struct StageArgsM {
+  const double* in;   // MODE_RHS input state
+  double* outd;       // MODE_RHS output derivative (FP64)
+  float* out;         // MODE_STAGE output derivative
+  double* U[2];
+  float* K1[2];
+  float* K2;
+  float* K3;
+  int kin_k2;
+  double coef;
+  const CtrlState* ctrl;
+  double* partials;
+};
+
 namespace dev {
 // Launchers (one translation unit per arithmetic mode).
 cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
@@ -72,6 +87,9 @@ cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A,
                               cudaStream_t s);
 cudaError_t prepare_fused_exact();
 cudaError_t prepare_fused_fast();
+cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A,
+                               cudaStream_t s);
+cudaError_t prepare_fused_mixed();
 int fused_grid_blocks(int Nx, int Ny);
 size_t fused_smem_bytes();
 

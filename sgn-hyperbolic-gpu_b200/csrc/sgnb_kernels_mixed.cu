@@ -1,0 +1,38 @@
+// sgnb_kernels_mixed.cu -- mixed-precision fused kernels (FP32 deviations, FP64
+// hydrostatic balance, state and controller). Built with -fmad=true.
+#include "sgnb_kernels_mixed.cuh"
+
+namespace sgnb {
+namespace dev {
+
+template <int MODE>
+static cudaError_t launch_m(const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
+  const dim3 grid((C.Nx + mix::TX - 1) / mix::TX, (C.Ny + mix::TY - 1) / mix::TY);
+  mix::k_mixed<MODE><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
+  switch (mode) {
+    case 0: return launch_m<mix::MODE_RHS>(C, A, s);
+    case 1: return launch_m<mix::MODE_STAGE>(C, A, s);
+    case 2: return launch_m<mix::MODE_FSAL>(C, A, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t prepare_fused_mixed() {
+  const int bytes = (int)sizeof(mix::Smem);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_RHS>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_STAGE>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(mix::k_mixed<mix::MODE_FSAL>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+}  // namespace dev
+}  // namespace sgnb

@@ -1,0 +1,585 @@
+// sgnb_kernels_mixed.cuh -- mixed-precision variant of the fused right-hand side and
+// BS3(2) stage kernels.
+//
+// Precision split (every term of src/physics/sgn_flux2d.h appears in exactly one part):
+//   FP64  the well-balanced hydrostatic flux 0.5 g (h^2 - H^2) of the normal momentum, its
+//         Rusanov central average, its FR-corrected derivative, and the bathymetry source
+//         g (h - H) grad H. These two cancel to O(g h grad eta); the cancellation happens
+//         in FP64 and only the result is rounded to FP32. The state, the RK stage
+//         combinations, the embedded error estimate and the controller are FP64 too.
+//   FP32  everything that is a deviation from the lake at rest: mass and advective
+//         fluxes, the hp and hw fluxes, Rusanov dissipation lam/2 (U_R - U_L) (the jump of h
+//         is formed in FP64 and rounded), wave speeds, the FR derivatives of these fluxes,
+//         the depth gradient D eta + grad H of the non-conservative products, and the
+//         sources gamma p grad H, gamma p, -2 c^2 (w + u H_x + v H_y).
+// At rest every FP32 term is exactly zero, so the lake-at-rest residual is the FP64 one.
+// Stage derivatives k are stored in FP32 (the RK accumulation u + dt sum b_i k_i and the
+// error estimate promote them to FP64).
+//
+// Layout and work decomposition are those of sgnb_kernels.cuh (8 x 4 element tiles, 5 warps,
+// lane = element, warp = GLL line); shared memory is 63 KB, so 3 CTAs fit per SM.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sgnb_device.h"
+
+namespace sgnb {
+namespace mix {
+
+constexpr int NP = 5, NPP = 25, NV = 5;
+constexpr int TX = 8, TY = 4, TE = TX * TY;
+constexpr int NWARP = 5, NTHR = 32 * NWARP;
+constexpr int NHALO = 2 * TY + 2 * TX;
+constexpr int RUN = TX * NPP;
+constexpr int NIT = TY * RUN / NTHR;
+constexpr int NHIT = (NV * NHALO * NP + NTHR - 1) / NTHR;
+constexpr int NFACE = (2 * TE + TY + TX) * NP;
+constexpr int NFIT = (NFACE + NTHR - 1) / NTHR;
+
+enum : int { MODE_RHS = 0, MODE_STAGE = 1, MODE_FSAL = 2 };
+
+struct Smem {
+  double h[TE][NPP];          // full depth (FP64)
+  double H[TE][NPP];          // nodal still depth
+  double Hx[TE][NPP];
+  double Hy[TE][NPP];
+  float q[4][TE][NPP];        // hu, hv, hw, hp (FP32 deviations)
+  float G[NV + 1][TE][NPP];   // column-pass results (dG incl. the y hydrostatic part, By)
+  double hhalo[NHALO * NP];   // halo depth, slot layout of sgnb_kernels.cuh
+  float qhalo[4 * NHALO * NP];
+  double Hf[(2 * TE + TY + TX) * NP];
+  double red[NWARP][3];
+};
+
+__device__ __forceinline__ double& hf_x(Smem& S, int i, int t) { return S.Hf[i * NP + t]; }
+__device__ __forceinline__ double& hf_y(Smem& S, int i, int t) { return S.Hf[(TE + i) * NP + t]; }
+__device__ __forceinline__ double& hf_xr(Smem& S, int iy, int t) { return S.Hf[(2 * TE + iy) * NP + t]; }
+__device__ __forceinline__ double& hf_yt(Smem& S, int ix, int t) { return S.Hf[(2 * TE + TY + ix) * NP + t]; }
+
+struct StageInM {
+  const double* __restrict__ in;
+  const double* __restrict__ u;
+  const float* __restrict__ k;
+  const float* __restrict__ k1;
+  const float* __restrict__ k2;
+  const float* __restrict__ k3;
+  double acoef, dt;
+};
+
+// FP64 stage input (src/solver/rk.cpp:100-108 with FP32 derivatives promoted).
+template <int MODE>
+__device__ __forceinline__ double stage_value(const StageInM& I, long long idx) {
+  if constexpr (MODE == MODE_RHS) {
+    return I.in[idx];
+  } else if constexpr (MODE == MODE_STAGE) {
+    return I.u[idx] + I.acoef * (double)I.k[idx];
+  } else {
+    return I.u[idx] + I.dt * (2.0 / 9.0 * (double)I.k1[idx] + 1.0 / 3.0 * (double)I.k2[idx] +
+                              4.0 / 9.0 * (double)I.k3[idx]);
+  }
+}
+
+// One point as seen by the FP32 part.
+struct PtF {
+  float h, hn, hu, hv, hw, hp;  // full depth (rounded), normal discharge, discharges
+  float u, v, w, p;             // primitives
+};
+
+template <int DIR>
+__device__ __forceinline__ PtF make_pt(double h64, float hu, float hv, float hw, float hp) {
+  PtF s;
+  s.h = (float)h64;
+  s.hu = hu; s.hv = hv; s.hw = hw; s.hp = hp;
+  s.hn = DIR == 0 ? hu : hv;
+  const float r = __fdividef(1.0f, s.h);
+  s.u = hu * r; s.v = hv * r; s.w = hw * r; s.p = hp * r;
+  return s;
+}
+
+// FP32 (deviation) part of flux field v; the hydrostatic term is added in FP64 elsewhere.
+template <int DIR>
+__device__ __forceinline__ float flux_dev(const RhsConsts& C, int v, const PtF& s) {
+  switch (v) {
+    case 0: return s.hn;
+    case 1: return DIR == 0 ? s.hu * s.u + s.hp : s.hv * s.u;
+    case 2: return DIR == 0 ? s.hu * s.v : s.hv * s.v + s.hp;
+    case 3: return s.hn * s.w;
+    default: return s.hn * (s.p + (float)C.c2);
+  }
+}
+
+template <int DIR>
+__device__ __forceinline__ float wave_speed_f(const RhsConsts& C, const PtF& s) {
+  const float arg = (float)C.g * s.h + s.p + (float)C.c2;
+  return fabsf(DIR == 0 ? s.u : s.v) + sqrtf(fmaxf(arg, 0.0f));
+}
+
+// Hydrostatic part of the normal momentum flux, FP64: 0.5 g (h^2 - H^2) as
+// 0.5 g (h - H)(h + H), which is exact at rest and cancels no digits.
+__device__ __forceinline__ double hydro64(const RhsConsts& C, double h, double Hl) {
+  return C.halfg * ((h - Hl) * (h + Hl));
+}
+
+// One GLL line: dyn[5] (FP32 FR derivatives of the deviation fluxes), hyd (FP64 FR
+// derivative of the hydrostatic flux of the normal momentum) and deta (FP32 FR derivative
+// of the depth with the central face depth). Emitted per node through the callbacks.
+//   h[k]      full depth at the nodes (FP64), Hn[k] nodal still depth
+//   qf[k][4]  FP32 hu, hv, hw, hp at the nodes
+//   nh, nq    the neighbour node across each face (FP64 depth, FP32 discharges)
+template <int DIR, class EmitN, class Emit>
+__device__ __forceinline__ void line_mixed(const RhsConsts& C, const double (&h)[NP],
+                                           const double (&Hn)[NP], const float (&qf)[NP][4],
+                                           double nhLo, const float* nqLo, double nhHi,
+                                           const float* nqHi, double HfLo, double HfHi,
+                                           EmitN&& emit_node, Emit&& emit) {
+  PtF s[NP];
+  float eta[NP];
+  double hyd[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    s[k] = make_pt<DIR>(h[k], qf[k][0], qf[k][1], qf[k][2], qf[k][3]);
+    eta[k] = (float)(h[k] - Hn[k]);
+    hyd[k] = hydro64(C, h[k], Hn[k]);
+  }
+  const PtF sLo = make_pt<DIR>(nhLo, nqLo[0], nqLo[1], nqLo[2], nqLo[3]);
+  const PtF sHi = make_pt<DIR>(nhHi, nqHi[0], nqHi[1], nqHi[2], nqHi[3]);
+  const PtF& tLo = s[0];
+  const PtF& tHi = s[NP - 1];
+  // Rusanov, FP32 deviation part (sgn_flux2d.h:169-179)
+  const float lamLo = fmaxf(wave_speed_f<DIR>(C, sLo), wave_speed_f<DIR>(C, tLo));
+  const float lamHi = fmaxf(wave_speed_f<DIR>(C, tHi), wave_speed_f<DIR>(C, sHi));
+  // jumps of the conserved variables: h in FP64, rounded after the difference
+  const float dhLo = (float)(h[0] - nhLo), dhHi = (float)(nhHi - h[NP - 1]);
+  float jLo[NV], jHi[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const float FdLo = flux_dev<DIR>(C, v, tLo), FdHi = flux_dev<DIR>(C, v, tHi);
+    const float FnLo = flux_dev<DIR>(C, v, sLo), FnHi = flux_dev<DIR>(C, v, sHi);
+    float duLo, duHi;  // own minus neighbour (low face), neighbour minus own (high face)
+    switch (v) {
+      case 0: duLo = dhLo; duHi = dhHi; break;
+      case 1: duLo = tLo.hu - sLo.hu; duHi = sHi.hu - tHi.hu; break;
+      case 2: duLo = tLo.hv - sLo.hv; duHi = sHi.hv - tHi.hv; break;
+      case 3: duLo = tLo.hw - sLo.hw; duHi = sHi.hw - tHi.hw; break;
+      default: duLo = tLo.hp - sLo.hp; duHi = sHi.hp - tHi.hp; break;
+    }
+    jLo[v] = 0.5f * (FnLo - FdLo) - 0.5f * lamLo * duLo;
+    jHi[v] = 0.5f * (FnHi - FdHi) - 0.5f * lamHi * duHi;
+  }
+  // hydrostatic jumps at the faces (FP64): central average minus own face value
+  const double jHydLo = 0.5 * (hydro64(C, nhLo, HfLo) - hydro64(C, h[0], HfLo));
+  const double jHydHi = 0.5 * (hydro64(C, nhHi, HfHi) - hydro64(C, h[NP - 1], HfHi));
+  // depth jumps with the central common depth h* = (h- + h+)/2 (sgn2d.cpp:213-214)
+  const float jeLo = -0.5f * dhLo, jeHi = 0.5f * dhHi;
+  const float iJ = (float)(DIR == 0 ? C.iJx : C.iJy);
+  const double iJ64 = DIR == 0 ? C.iJx : C.iJy;
+#pragma unroll
+  for (int m = 0; m < NP; ++m) {
+    const float gL = (float)C.gLp[m], gR = (float)C.gRp[m];
+    float se = jeLo * gL + jeHi * gR;
+    double sh = jHydLo * C.gLp[m] + jHydHi * C.gRp[m];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      se = fmaf((float)C.D[m * NP + k], eta[k], se);
+      sh = fma(C.D[m * NP + k], hyd[k], sh);
+    }
+    emit_node(m, se * iJ, sh * iJ64, s[m], eta[m]);
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    float F[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) F[k] = flux_dev<DIR>(C, v, s[k]);
+#pragma unroll
+    for (int m = 0; m < NP; ++m) {
+      float a = jLo[v] * (float)C.gLp[m];
+      a = fmaf(jHi[v], (float)C.gRp[m], a);
+#pragma unroll
+      for (int k = 0; k < NP; ++k) a = fmaf((float)C.D[m * NP + k], F[k], a);
+      emit(m, v, a * iJ, s[m]);
+    }
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const StageArgsM A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+
+  int cur = 0;
+  double atol = 0.0, rtol = 0.0;
+  StageInM I;
+  I.in = A.in;
+  I.dt = 0.0;
+  I.acoef = 0.0;
+  if constexpr (MODE != MODE_RHS) {
+    if (A.ctrl->done) return;
+    cur = A.ctrl->cur;
+    I.dt = A.ctrl->dt;
+    I.acoef = A.coef * I.dt;
+    atol = A.ctrl->atol;
+    rtol = A.ctrl->rtol;
+  }
+  I.u = A.U[cur];
+  I.k = A.kin_k2 ? A.K2 : A.K1[cur];
+  I.k1 = A.K1[cur];
+  I.k2 = A.K2;
+  I.k3 = A.K3;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int Nx = C.Nx, Ny = C.Ny;
+  const long long Nd = C.Nd;
+  const int ex0 = blockIdx.x * TX, ey0 = blockIdx.y * TY;
+  const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
+  const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
+  const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
+
+  long long gof[NIT];
+  int sof[NIT];
+  bool okk[NIT];
+  auto item_map = [&]() {
+#pragma unroll
+    for (int u = 0; u < NIT; ++u) {
+      const int q = tid + NTHR * u;
+      const int iy = q / RUN, k = q - iy * RUN;
+      okk[u] = iy < TYv && k < TXv * NPP;
+      gof[u] = ((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k;
+      sof[u] = iy * RUN + k;
+    }
+  };
+  item_map();
+
+  // ---- load phase ----------------------------------------------------------------
+  {
+    double a0[NIT], a1[NIT], a2[NIT];
+#pragma unroll
+    for (int u = 0; u < NIT; ++u)
+      if (okk[u]) { a0[u] = C.Hnod[gof[u]]; a1[u] = C.Hx[gof[u]]; a2[u] = C.Hy[gof[u]]; }
+#pragma unroll
+    for (int u = 0; u < NIT; ++u)
+      if (okk[u]) {
+        (&S.H[0][0])[sof[u]] = a0[u];
+        (&S.Hx[0][0])[sof[u]] = a1[u];
+        (&S.Hy[0][0])[sof[u]] = a2[u];
+      }
+    double* __restrict__ unew = A.U[cur ^ 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double x[NIT];
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          if (v == 0) (&S.h[0][0])[sof[u]] = x[u];
+          else (&S.q[v - 1][0][0])[sof[u]] = (float)x[u];
+          if constexpr (MODE == MODE_FSAL) unew[(long long)v * Nd + gof[u]] = x[u];
+        }
+    }
+    // halos
+    double hv[NHIT];
+    int hq[NHIT];
+    long long hg[NHIT];
+#pragma unroll
+    for (int u = 0; u < NHIT; ++u) {
+      const int q = tid + NTHR * u;
+      const int t = q % NP, r = q / NP;
+      const int slot = r % NHALO, v = r / NHALO;
+      bool ok = q < NV * NHALO * NP;
+      long long e = 0;
+      int node = 0;
+      if (slot < TY) {
+        ok = ok && slot < TYv && !wallL;
+        e = (long long)((ex0 - 1 + Nx) % Nx) + (long long)Nx * (ey0 + slot);
+        node = (NP - 1) + NP * t;
+      } else if (slot < 2 * TY) {
+        ok = ok && slot - TY < TYv && !wallR;
+        e = (long long)((ex0 + TXv) % Nx) + (long long)Nx * (ey0 + slot - TY);
+        node = NP * t;
+      } else if (slot < 2 * TY + TX) {
+        ok = ok && slot - 2 * TY < TXv && !wallB;
+        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * ((ey0 - 1 + Ny) % Ny);
+        node = t + NP * (NP - 1);
+      } else {
+        ok = ok && slot - 2 * TY - TX < TXv && !wallT;
+        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * ((ey0 + TYv) % Ny);
+        node = t;
+      }
+      hq[u] = ok ? q : -1;
+      hg[u] = (long long)v * Nd + e * NPP + node;
+    }
+#pragma unroll
+    for (int u = 0; u < NHIT; ++u)
+      if (hq[u] >= 0) hv[u] = stage_value<MODE>(I, hg[u]);
+    double fv[NFIT];
+    int fq[NFIT];
+#pragma unroll
+    for (int u = 0; u < NFIT; ++u) {
+      const int q = tid + NTHR * u;
+      fq[u] = -1;
+      if (q < 2 * TE * NP) {
+        const int t = q % NP, i = (q / NP) % TE, s = q / (NP * TE);
+        const int ix = i % TX, iy = i / TX;
+        if (ix < TXv && iy < TYv) {
+          const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
+          fv[u] = (s == 0 ? C.HfX : C.HfY)[e * NP + t];
+          fq[u] = q;
+        }
+      } else if (q < NFACE) {
+        const int r = q - 2 * TE * NP;
+        const int t = r % NP, slot = r / NP;
+        if (slot < TY) {
+          if (slot < TYv) {
+            const int ey = ey0 + slot;
+            fv[u] = wallR ? C.HfXEnd[(long long)ey * NP + t]
+                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
+            fq[u] = q;
+          }
+        } else if (slot - TY < TXv) {
+          const int ex = ex0 + slot - TY;
+          fv[u] = wallT ? C.HfYEnd[(long long)ex * NP + t]
+                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t];
+          fq[u] = q;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < NHIT; ++u)
+      if (hq[u] >= 0) {
+        const int q = hq[u];
+        const int v = q / (NHALO * NP), rest = q - v * NHALO * NP;
+        if (v == 0) S.hhalo[rest] = hv[u];
+        else S.qhalo[(v - 1) * NHALO * NP + rest] = (float)hv[u];
+      }
+#pragma unroll
+    for (int u = 0; u < NFIT; ++u)
+      if (fq[u] >= 0) S.Hf[fq[u]] = fv[u];
+  }
+  __syncthreads();
+
+  const int i = lane;
+  const int ix = i % TX, iy = i / TX;
+  const bool valid = ix < TXv && iy < TYv;
+  const int j = warp;
+  const float c2f = (float)C.c2, mc2f = (float)C.mc2, gammaf = (float)C.gamma;
+
+  // neighbour node across a face: in the tile, in the halo, or the wall mirror
+  auto halo_node = [&](int slot, int t, double& hh, float* qq) {
+    const int idx = t + NP * slot;
+    hh = S.hhalo[idx];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qq[c] = S.qhalo[c * NHALO * NP + idx];
+  };
+  auto tile_node = [&](int e, int loc, double& hh, float* qq) {
+    hh = S.h[e][loc];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qq[c] = S.q[c][e][loc];
+  };
+
+  // ---- column pass: y-line a = j ---------------------------------------------
+  if (valid) {
+    double h[NP], Hn[NP];
+    float qf[NP][4];
+#pragma unroll
+    for (int b = 0; b < NP; ++b) {
+      const int loc = j + NP * b;
+      h[b] = S.h[i][loc];
+      Hn[b] = S.H[i][loc];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) qf[b][c] = S.q[c][i][loc];
+    }
+    double nhLo, nhHi;
+    float nqLo[4], nqHi[4];
+    if (iy > 0) tile_node(i - TX, j + NP * (NP - 1), nhLo, nqLo);
+    else if (wallB) {
+      nhLo = h[0];
+      nqLo[0] = qf[0][0]; nqLo[1] = -qf[0][1]; nqLo[2] = qf[0][2]; nqLo[3] = qf[0][3];
+    } else halo_node(2 * TY + ix, j, nhLo, nqLo);
+    if (iy + 1 < TYv) tile_node(i + TX, j, nhHi, nqHi);
+    else if (wallT) {
+      nhHi = h[NP - 1];
+      nqHi[0] = qf[NP - 1][0]; nqHi[1] = -qf[NP - 1][1]; nqHi[2] = qf[NP - 1][2]; nqHi[3] = qf[NP - 1][3];
+    } else halo_node(2 * TY + TX + ix, j, nhHi, nqHi);
+    const double HfLo = hf_y(S, i, j);
+    const double HfHi = (iy + 1 < TYv) ? hf_y(S, i + TX, j) : hf_yt(S, ix, j);
+    float hydv[NP];
+    line_mixed<1>(
+        C, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
+        [&](int b, float deta, double dhyd, const PtF& s, float) {
+          const int loc = j + NP * b;
+          const double Hyl = S.Hy[i][loc];
+          // ncpY with h_y = D eta + H_y (sgn_flux2d.h:156-161)
+          S.G[NV][i][loc] = mc2f * s.v * (deta + (float)Hyl);
+          // y hydrostatic part of dU[HV]: -d_y hyd + g (h - H) H_y, cancelled in FP64
+          hydv[b] = (float)(C.g * (h[b] - Hn[b]) * Hyl - dhyd);
+        },
+        [&](int b, int v, float d, const PtF&) {
+          S.G[v][i][j + NP * b] = (v == 2) ? d - hydv[b] : d;
+        });
+  }
+  __syncthreads();
+
+  // ---- row pass: x-line b = j, then assembly ---------------------------------
+  if (valid) {
+    double h[NP], Hn[NP];
+    float qf[NP][4];
+#pragma unroll
+    for (int a = 0; a < NP; ++a) {
+      const int loc = a + NP * j;
+      h[a] = S.h[i][loc];
+      Hn[a] = S.H[i][loc];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) qf[a][c] = S.q[c][i][loc];
+    }
+    double nhLo, nhHi;
+    float nqLo[4], nqHi[4];
+    if (ix > 0) tile_node(i - 1, (NP - 1) + NP * j, nhLo, nqLo);
+    else if (wallL) {
+      nhLo = h[0];
+      nqLo[0] = -qf[0][0]; nqLo[1] = qf[0][1]; nqLo[2] = qf[0][2]; nqLo[3] = qf[0][3];
+    } else halo_node(iy, j, nhLo, nqLo);
+    if (ix + 1 < TXv) tile_node(i + 1, NP * j, nhHi, nqHi);
+    else if (wallR) {
+      nhHi = h[NP - 1];
+      nqHi[0] = -qf[NP - 1][0]; nqHi[1] = qf[NP - 1][1]; nqHi[2] = qf[NP - 1][2]; nqHi[3] = qf[NP - 1][3];
+    } else halo_node(TY + iy, j, nhHi, nqHi);
+    const double HfLo = hf_x(S, i, j);
+    const double HfHi = (ix + 1 < TXv) ? hf_x(S, i + 1, j) : hf_xr(S, iy, j);
+    float hydu[NP], Bx[NP];
+    line_mixed<0>(
+        C, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
+        [&](int a, float deta, double dhyd, const PtF& s, float) {
+          const int loc = a + NP * j;
+          const double Hxl = S.Hx[i][loc];
+          Bx[a] = mc2f * s.u * (deta + (float)Hxl);  // ncpX
+          hydu[a] = (float)(C.g * (h[a] - Hn[a]) * Hxl - dhyd);
+        },
+        [&](int a, int v, float d, const PtF& s) {
+          const int loc = a + NP * j;
+          const float g = S.G[v][i][loc];
+          float res;
+          if (v == 0) {
+            res = -(d + g);
+          } else if (v == 1) {
+            res = hydu[a] + gammaf * s.p * (float)S.Hx[i][loc] - (d + g);
+          } else if (v == 2) {
+            res = gammaf * s.p * (float)S.Hy[i][loc] - (d + g);
+          } else if (v == 3) {
+            res = gammaf * s.p - (d + g);
+          } else {
+            const float Hxl = (float)S.Hx[i][loc], Hyl = (float)S.Hy[i][loc];
+            const float S4 = (float)C.m2c2 * (s.w + s.u * Hxl + s.v * Hyl);
+            res = S4 - (d + g) - Bx[a] - S.G[NV][i][loc];
+          }
+          S.G[v][i][loc] = res;
+        });
+  }
+  __syncthreads();
+
+  // ---- copy-out and the FP64 embedded error of the end-point stage ---------------
+  double esum = 0.0, emax = 0.0;
+  int enan = 0;
+  item_map();
+  if constexpr (MODE == MODE_RHS) {
+    // FP64 output for rhs callers, FP32 into the stage buffer for the FSAL head
+#pragma unroll 1
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          const float val = (&S.G[v][0][0])[sof[u]];
+          if (A.outd) A.outd[(long long)v * Nd + gof[u]] = (double)val;
+          else A.out[(long long)v * Nd + gof[u]] = val;
+        }
+  } else if constexpr (MODE == MODE_STAGE) {
+#pragma unroll 1
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) A.out[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
+  } else {
+    const volatile CtrlState* vc = A.ctrl;
+    cur = vc->cur;
+    const double dt = vc->dt;
+    atol = vc->atol;
+    rtol = vc->rtol;
+    const double* __restrict__ u0 = A.U[cur];
+    const float* __restrict__ k1p = A.K1[cur];
+    const float* __restrict__ k2p = A.K2;
+    const float* __restrict__ k3p = A.K3;
+    float* __restrict__ outp = A.K1[cur ^ 1];
+    // next field's u, k1, k2, k3 prefetched while the current field's error is formed
+    double uu[NIT], nu[NIT];
+    float c1[NIT], c2[NIT], c3[NIT], n1[NIT], n2[NIT], n3[NIT];
+#pragma unroll
+    for (int u = 0; u < NIT; ++u)
+      if (okk[u]) {
+        const long long g = gof[u];
+        uu[u] = u0[g]; c1[u] = k1p[g]; c2[u] = k2p[g]; c3[u] = k3p[g];
+      }
+#pragma unroll 1
+    for (int v = 0; v < NV; ++v) {
+      if (v + 1 < NV) {
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            const long long g = (long long)(v + 1) * Nd + gof[u];
+            nu[u] = u0[g]; n1[u] = k1p[g]; n2[u] = k2p[g]; n3[u] = k3p[g];
+          }
+      }
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          const float k4 = (&S.G[v][0][0])[sof[u]];
+          outp[(long long)v * Nd + gof[u]] = k4;
+          const double b1 = c1[u], b2 = c2[u], b3 = c3[u], b4 = k4;
+          const double un = uu[u] + dt * (2.0 / 9.0 * b1 + 1.0 / 3.0 * b2 + 4.0 / 9.0 * b3);
+          const double uEmb = uu[u] + dt * (7.0 / 24.0 * b1 + 0.25 * b2 + 1.0 / 3.0 * b3 + 0.125 * b4);
+          const double e = un - uEmb;
+          const double au = fabs(uu[u]), an = fabs(un);
+          const double sc = atol + rtol * (au < an ? an : au);
+          const double rr = e / sc;
+          esum += rr * rr;
+          const double ar = fabs(rr);
+          emax = emax < ar ? ar : emax;
+          enan |= (rr != rr);
+        }
+#pragma unroll
+      for (int u = 0; u < NIT; ++u) {
+        uu[u] = nu[u]; c1[u] = n1[u]; c2[u] = n2[u]; c3[u] = n3[u];
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      esum += __shfl_down_sync(0xffffffffu, esum, off);
+      const double om = __shfl_down_sync(0xffffffffu, emax, off);
+      emax = emax < om ? om : emax;
+      enan |= __shfl_down_sync(0xffffffffu, enan, off);
+    }
+    if (lane == 0) {
+      S.red[warp][0] = esum;
+      S.red[warp][1] = emax;
+      S.red[warp][2] = (double)enan;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0, m = 0.0, n = 0.0;
+      for (int w = 0; w < NWARP; ++w) {
+        s += S.red[w][0];
+        m = m < S.red[w][1] ? S.red[w][1] : m;
+        n += S.red[w][2];
+      }
+      const long long blk = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+      A.partials[3 * blk + 0] = s;
+      A.partials[3 * blk + 1] = m;
+      A.partials[3 * blk + 2] = n;
+    }
+  }
+}
+
+}  // namespace mix
+}  // namespace sgnb

@@ -30,6 +30,7 @@ BC_PERIODIC = 0
 BC_WALL = 1
 FP64_EXACT = 0
 FP64_FAST = 1
+MIXED = 2
 
 BATHY_NONE = 0
 BATHY_CONST = 1

@@ -111,3 +111,23 @@ def cfg2_case(Nx=2048, Ny=1024, Lx=40.0, Ly=20.0, seed=2, chunk=1 << 22):
             eta += a * np.sin(k * (xs * np.cos(t) + ys * np.sin(t)) + ph)
         U[s:s + xs.size] = H + eta
     return kw, U
+
+
+def cfg3_bathymetry(seed=3, Lx=20.0, Ly=10.0, H0=1.0):
+    """Configuration 3's lake-at-rest bathymetry: H0 minus 5 seeded Gaussian bumps of
+    height 0.05-0.3, centres uniform in the domain, widths sigma in [0.5, 2]
+    (BATHY_GAUSS_SUM parameters)."""
+    rng = np.random.default_rng(seed)
+    par = [H0, 5]
+    for _ in range(5):
+        par += [rng.uniform(0.05, 0.3), rng.uniform(0, Lx), rng.uniform(0, Ly),
+                rng.uniform(0.5, 2.0)]
+    return tuple(par)
+
+
+def cfg3_lake_case():
+    Nx, Ny, Lx, Ly = 128, 64, 20.0, 10.0
+    kw = dict(P=4, Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, g=G, c=ALPHA * np.sqrt(G * 1.0), gamma=GAMMA,
+              bc_x=BC_PERIODIC, bc_y=BC_PERIODIC, bathy_kind=BATHY_GAUSS_SUM,
+              bathy_par=cfg3_bathymetry())
+    return kw
