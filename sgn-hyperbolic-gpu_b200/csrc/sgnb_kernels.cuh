@@ -94,6 +94,16 @@ __device__ __forceinline__ double& halo_at(Smem& S, int v, int slot, int t) {
   return S.halo[t + NP * (slot + NHALO * v)];
 }
 
+// Asynchronous global -> shared copy of one double (cp.async, no register staging), and
+// the wait for all of this thread's outstanding copies.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // Read-only views of the stage inputs of one launch.
 struct StageIn {
   const double* __restrict__ in;
@@ -105,16 +115,28 @@ struct StageIn {
   double acoef, dt;
 };
 
+// Stage combinations of src/solver/rk.cpp:100-108, with every product and sum rounded on
+// its own in both arithmetic modes: a tile forms its own nodes in shared memory and its
+// neighbours' halo nodes in registers, and the two must agree bit for bit.
+__device__ __forceinline__ double stage_axpy(double u, double acoef, double k) {
+  return __dadd_rn(u, __dmul_rn(acoef, k));  // u + (c dt) k
+}
+__device__ __forceinline__ double fsal_part(double k1, double k2) {
+  return __dadd_rn(__dmul_rn(2.0 / 9.0, k1), __dmul_rn(1.0 / 3.0, k2));  // 2/9 k1 + 1/3 k2
+}
+__device__ __forceinline__ double fsal_finish(double u, double part, double k3, double dt) {
+  return __dadd_rn(u, __dmul_rn(dt, __dadd_rn(part, __dmul_rn(4.0 / 9.0, k3))));
+}
+
 // Stage input of one value: plain, u + (coef dt) k, or the BS3 candidate.
-// Expression trees follow src/solver/rk.cpp:100-108 exactly.
 template <int MODE>
 __device__ __forceinline__ double stage_value(const StageIn& I, long long idx) {
   if constexpr (MODE == MODE_RHS) {
     return I.in[idx];
   } else if constexpr (MODE == MODE_STAGE) {
-    return I.u[idx] + I.acoef * I.k[idx];
+    return stage_axpy(I.u[idx], I.acoef, I.k[idx]);
   } else {
-    return I.u[idx] + I.dt * (2.0 / 9.0 * I.k1[idx] + 1.0 / 3.0 * I.k2[idx] + 4.0 / 9.0 * I.k3[idx]);
+    return fsal_finish(I.u[idx], fsal_part(I.k1[idx], I.k2[idx]), I.k3[idx], I.dt);
   }
 }
 
@@ -394,36 +416,38 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
 
   // ---- load phase --------------------------------------------------------------
   {
-    // statics: all loads first, then the shared-memory stores
-    const double* __restrict__ gH = C.Hnod;
-    const double* __restrict__ gHx = C.Hx;
-    const double* __restrict__ gHy = C.Hy;
-    double a0[NIT], a1[NIT], a2[NIT];
-#pragma unroll
-    for (int u = 0; u < NIT; ++u)
-      if (okk[u]) { a0[u] = gH[gof[u]]; a1[u] = gHx[gof[u]]; a2[u] = gHy[gof[u]]; }
-    // statics to shared memory first: they are not needed in registers
+    // Statics, and the state of the rhs and stage modes, arrive by asynchronous copies
+    // straight into shared memory: a tile's loads are all in flight at once without
+    // holding registers. The stage mode stages k in the (still unused) G area and forms
+    // u + (c dt) k in shared memory once the copies have landed.
 #pragma unroll
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
-        (&S.H[0][0])[sof[u]] = a0[u];
-        (&S.Hx[0][0])[sof[u]] = a1[u];
-        (&S.Hy[0][0])[sof[u]] = a2[u];
+        cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+        cp_async8(&(&S.Hx[0][0])[sof[u]], C.Hx + gof[u]);
+        cp_async8(&(&S.Hy[0][0])[sof[u]], C.Hy + gof[u]);
       }
-    // state: field by field, all items' loads of a field in flight together
-    double* __restrict__ unew = A.U[cur ^ 1];
+    if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) {
+      const double* __restrict__ src = MODE == MODE_RHS ? I.in : I.u;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      double x[NIT];
+      for (int v = 0; v < NV; ++v)
 #pragma unroll
-      for (int u = 0; u < NIT; ++u)
-        if (okk[u]) x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            cp_async8(&(&S.U[v][0][0])[sof[u]], src + (long long)v * Nd + gof[u]);
+            if constexpr (MODE == MODE_STAGE)
+              cp_async8(&(&S.G[v][0][0])[sof[u]], I.k + (long long)v * Nd + gof[u]);
+          }
+    } else {
+      // end-point stage, round 1: k1 and k2 into the U and G areas
 #pragma unroll
-      for (int u = 0; u < NIT; ++u)
-        if (okk[u]) {
-          (&S.U[v][0][0])[sof[u]] = x[u];
-          if constexpr (MODE == MODE_FSAL) unew[(long long)v * Nd + gof[u]] = x[u];
-        }
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            cp_async8(&(&S.U[v][0][0])[sof[u]], I.k1 + (long long)v * Nd + gof[u]);
+            cp_async8(&(&S.G[v][0][0])[sof[u]], I.k2 + (long long)v * Nd + gof[u]);
+          }
     }
     // halo items: descriptors, then loads
     double hv[NHIT];
@@ -499,6 +523,48 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
 #pragma unroll
     for (int u = 0; u < NFIT; ++u)
       if (fq[u] >= 0) S.Hf[fq[u]] = fv[u];
+    cp_async_wait_all();
+    if constexpr (MODE == MODE_STAGE) {
+      // u + (c dt) k for this thread's own items (rk.cpp:100-103), in shared memory
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            double& y = (&S.U[v][0][0])[sof[u]];
+            y = stage_axpy(y, I.acoef, (&S.G[v][0][0])[sof[u]]);
+          }
+    } else if constexpr (MODE == MODE_FSAL) {
+      // round 2: 2/9 k1 + 1/3 k2 in place, k3 into the G area while u comes through
+      // registers, then uNew = u + dt ((2/9 k1 + 1/3 k2) + 4/9 k3) (rk.cpp:106-108),
+      // written to shared memory and out as the candidate state
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            double& y = (&S.U[v][0][0])[sof[u]];
+            y = fsal_part(y, (&S.G[v][0][0])[sof[u]]);
+            cp_async8(&(&S.G[v][0][0])[sof[u]], I.k3 + (long long)v * Nd + gof[u]);
+          }
+      double* __restrict__ unew = A.U[cur ^ 1];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        double x[NIT];
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) x[u] = I.u[(long long)v * Nd + gof[u]];
+        if (v == 0) cp_async_wait_all();
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            double& y = (&S.U[v][0][0])[sof[u]];
+            const double un = fsal_finish(x[u], y, (&S.G[v][0][0])[sof[u]], I.dt);
+            y = un;
+            unew[(long long)v * Nd + gof[u]] = un;
+          }
+      }
+    }
   }
   __syncthreads();
 
@@ -665,7 +731,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
             outp[(long long)v * Nd + gof[u]] = k4;
             // scaled embedded error, src/solver/rk.cpp:118-128
             const double dt = I.dt;
-            const double un = uu[u] + dt * (2.0 / 9.0 * c1[u] + 1.0 / 3.0 * c2[u] + 4.0 / 9.0 * c3[u]);
+            const double un = fsal_finish(uu[u], fsal_part(c1[u], c2[u]), c3[u], dt);
             const double uEmb = uu[u] + dt * (7.0 / 24.0 * c1[u] + 0.25 * c2[u] + 1.0 / 3.0 * c3[u] +
                                               0.125 * k4);
             const double e = un - uEmb;

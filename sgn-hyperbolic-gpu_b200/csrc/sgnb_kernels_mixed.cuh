@@ -58,6 +58,14 @@ __device__ __forceinline__ double& hf_y(Smem& S, int i, int t) { return S.Hf[(TE
 __device__ __forceinline__ double& hf_xr(Smem& S, int iy, int t) { return S.Hf[(2 * TE + iy) * NP + t]; }
 __device__ __forceinline__ double& hf_yt(Smem& S, int ix, int t) { return S.Hf[(2 * TE + TY + ix) * NP + t]; }
 
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 struct StageInM {
   const double* __restrict__ in;
   const double* __restrict__ u;
@@ -254,24 +262,39 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
 
   // ---- load phase ----------------------------------------------------------------
   {
-    double a0[NIT], a1[NIT], a2[NIT];
-#pragma unroll
-    for (int u = 0; u < NIT; ++u)
-      if (okk[u]) { a0[u] = C.Hnod[gof[u]]; a1[u] = C.Hx[gof[u]]; a2[u] = C.Hy[gof[u]]; }
+    // statics by asynchronous copies straight into shared memory
 #pragma unroll
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
-        (&S.H[0][0])[sof[u]] = a0[u];
-        (&S.Hx[0][0])[sof[u]] = a1[u];
-        (&S.Hy[0][0])[sof[u]] = a2[u];
+        cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+        cp_async8(&(&S.Hx[0][0])[sof[u]], C.Hx + gof[u]);
+        cp_async8(&(&S.Hy[0][0])[sof[u]], C.Hy + gof[u]);
       }
     double* __restrict__ unew = A.U[cur ^ 1];
+    if constexpr (MODE == MODE_STAGE) {
+      // k (FP32) by asynchronous copies into the still unused G area
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) {
+            const unsigned sa = (unsigned)__cvta_generic_to_shared(&(&S.G[v][0][0])[sof[u]]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
+                         "l"(I.k + (long long)v * Nd + gof[u]) : "memory");
+          }
+      cp_async_wait_all();
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       double x[NIT];
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
-        if (okk[u]) x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
+        if (okk[u]) {
+          if constexpr (MODE == MODE_STAGE)
+            x[u] = I.u[(long long)v * Nd + gof[u]] + I.acoef * (double)(&S.G[v][0][0])[sof[u]];
+          else
+            x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
+        }
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
@@ -358,6 +381,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
 #pragma unroll
     for (int u = 0; u < NFIT; ++u)
       if (fq[u] >= 0) S.Hf[fq[u]] = fv[u];
+    cp_async_wait_all();
   }
   __syncthreads();
 
