@@ -360,6 +360,7 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   e = dev::prepare_fused_exact();
   if (e == cudaSuccess) e = dev::prepare_fused_fast();
   if (e == cudaSuccess) e = dev::prepare_fused_mixed();
+  if (e == cudaSuccess) e = dev::prepare_fused_batch();
   if (e != cudaSuccess) { cuda_fail(c, e, "kernel attributes"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
 
   // statics: Hnod, Hx, Hy (Nd each), HfX, HfY (5 ne each), HfXEnd (5 Ny), HfYEnd (5 Nx)
@@ -666,6 +667,380 @@ const char* sgnb_status_string(int s) {
 
 const char* sgnb_last_error(const sgnb_ctx* c) {
   return c ? c->err.c_str() : g_create_error.c_str();
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched sweep: many independent instances, one persistent launch per RK stage.
+// ===========================================================================
+constexpr int kTuneFactors = 4;  // persistent grids of 1..4 CTAs per SM
+
+struct sgnb_batch {
+  int n = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<sgnb_ctx*> ctx;          // per-instance buffers and statics
+  RhsConsts* dconsts = nullptr;        // [n]
+  StageArgs* dargs = nullptr;          // [n]
+  StageArgs* hargs = nullptr;          // pinned host mirror
+  CtrlState* dctrl = nullptr;          // [n]
+  CtrlState* hctrl = nullptr;          // pinned host mirror
+  double* dpartbuf = nullptr;          // error partials of every instance, 3 per tile
+  std::vector<double*> hpart;          // instance i's partials within dpartbuf
+  double** dpart = nullptr;            // [n] partial pointers
+  int* dnblk[3] = {nullptr, nullptr, nullptr};  // [n] tiles per instance, per tile shape
+  long long* dntot = nullptr;          // [n]
+  int* dtile_inst[3] = {nullptr, nullptr, nullptr};        // per tile shape
+  long long* dtile_start[3] = {nullptr, nullptr, nullptr};
+  long long ntiles[3] = {0, 0, 0};
+  int shape = 0;                       // tuned tile shape
+  int blocks = 0;                      // tuned persistent grid
+  cudaGraphExec_t chunk = nullptr;
+  int chunkShape = -1, chunkBlocks = -1;
+  cudaEvent_t evRead = nullptr;
+  long long launches = 0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(sgnb_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg; else g_create_error = msg;
+  return code;
+}
+
+#define SGNB_BCU(b, call)                                                    \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return bfail(b, e_ == cudaErrorMemoryAllocation ? SGNB_ERR_NOMEM : SGNB_ERR_CUDA, \
+                   std::string(#call) + ": " + cudaGetErrorName(e_));       \
+  } while (0)
+
+BatchArgs batch_args(sgnb_batch* b, int shape, int kin_k2, double coef) {
+  BatchArgs B{};
+  const RhsConsts& C0 = b->ctx[0]->C;
+  for (int k = 0; k < 25; ++k) B.tables.D[k] = C0.D[k];
+  for (int k = 0; k < 5; ++k) { B.tables.gLp[k] = C0.gLp[k]; B.tables.gRp[k] = C0.gRp[k]; }
+  B.consts = b->dconsts;
+  B.args = b->dargs;
+  B.tile_inst = b->dtile_inst[shape];
+  B.tile_start = b->dtile_start[shape];
+  B.ntiles = b->ntiles[shape];
+  B.kin_k2 = kin_k2;
+  B.coef = coef;
+  return B;
+}
+
+int batch_build_graph(sgnb_batch* b, int len) {
+  if (b->chunk && b->chunkShape == b->shape && b->chunkBlocks == b->blocks) return SGNB_OK;
+  if (b->chunk) { cudaGraphExecDestroy(b->chunk); b->chunk = nullptr; }
+  cudaGraph_t g = nullptr;
+  SGNB_BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < len && e == cudaSuccess; ++k) {
+    e = dev::launch_fused_batch(1, b->shape, b->blocks, batch_args(b, b->shape, 0, 0.5), b->stream);
+    if (e == cudaSuccess)
+      e = dev::launch_fused_batch(1, b->shape, b->blocks, batch_args(b, b->shape, 1, 0.75), b->stream);
+    if (e == cudaSuccess)
+      e = dev::launch_fused_batch(2, b->shape, b->blocks, batch_args(b, b->shape, 0, 0.0), b->stream);
+    if (e == cudaSuccess)
+      e = dev::launch_controller_batch(b->dctrl, b->dpart, b->dnblk[b->shape], b->dntot, b->n,
+                                       b->stream);
+  }
+  cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return bfail(b, SGNB_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorName(e)); }
+  if (e2 != cudaSuccess) return bfail(b, SGNB_ERR_CUDA, "batch cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&b->chunk, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return bfail(b, SGNB_ERR_CUDA, "batch cudaGraphInstantiate");
+  b->chunkShape = b->shape;
+  b->chunkBlocks = b->blocks;
+  return SGNB_OK;
+}
+
+bool all_done(const sgnb_batch* b) {
+  for (int i = 0; i < b->n; ++i)
+    if (!b->hctrl[i].done) return false;
+  return true;
+}
+
+// Stage arguments of every instance and the controllers (already initialised in
+// b->hctrl) to the device.
+int batch_prepare(sgnb_batch* b) {
+  for (int i = 0; i < b->n; ++i) {
+    sgnb_ctx* c = b->ctx[i];
+    StageArgs& A = b->hargs[i];
+    A = StageArgs{};
+    A.U[0] = c->U[0]; A.U[1] = c->U[1];
+    A.K1[0] = (double*)c->K1[0]; A.K1[1] = (double*)c->K1[1];
+    A.K2 = (double*)c->K2; A.K3 = (double*)c->K3;
+    A.ctrl = b->dctrl + i;
+    A.partials = b->hpart[i];
+    A.in = c->U[c->cur];          // FSAL head input and output
+    A.out = (double*)c->K1[c->cur];
+  }
+  SGNB_BCU(b, cudaMemcpyAsync(b->dargs, b->hargs, b->n * sizeof(StageArgs), cudaMemcpyHostToDevice, b->stream));
+  SGNB_BCU(b, cudaMemcpyAsync(b->dctrl, b->hctrl, b->n * sizeof(CtrlState), cudaMemcpyHostToDevice, b->stream));
+  return SGNB_OK;
+}
+
+// Controllers already initialised in b->hctrl; runs until every instance is done.
+int batch_run(sgnb_batch* b) {
+  const int len = 8;
+  if (int rc = batch_build_graph(b, len)) return rc;
+  if (int rc = batch_prepare(b)) return rc;
+  SGNB_BCU(b, dev::launch_fused_batch(0, b->shape, b->blocks, batch_args(b, b->shape, 0, 0.0), b->stream));
+  b->launches = 1 + 4LL * len;
+  SGNB_BCU(b, cudaGraphLaunch(b->chunk, b->stream));
+  SGNB_BCU(b, cudaMemcpyAsync(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost, b->stream));
+  SGNB_BCU(b, cudaEventRecord(b->evRead, b->stream));
+  for (;;) {
+    SGNB_BCU(b, cudaGraphLaunch(b->chunk, b->stream));
+    b->launches += 4LL * len;
+    SGNB_BCU(b, cudaEventSynchronize(b->evRead));
+    if (all_done(b)) break;
+    SGNB_BCU(b, cudaMemcpyAsync(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost, b->stream));
+    SGNB_BCU(b, cudaEventRecord(b->evRead, b->stream));
+  }
+  SGNB_BCU(b, cudaStreamSynchronize(b->stream));
+  SGNB_BCU(b, cudaMemcpy(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < b->n; ++i) b->ctx[i]->cur = b->hctrl[i].cur;
+  return SGNB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
+  if (!out || !descs || n < 1) return bfail(nullptr, SGNB_ERR_INVALID, "descs, n >= 1, out");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (descs[i].precision != SGNB_FP64_FAST)
+      return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run in SGNB_FP64_FAST");
+    if (descs[i].device != descs[0].device)
+      return bfail(nullptr, SGNB_ERR_INVALID, "all instances on one device");
+  }
+  sgnb_batch* b = new sgnb_batch();
+  b->n = n;
+  b->device = descs[0].device;
+  b->ctx.assign(n, nullptr);
+  for (int i = 0; i < n; ++i) {
+    int rc = sgnb_create(&descs[i], &b->ctx[i]);
+    if (rc) { sgnb_batch_destroy(b); return rc; }
+  }
+  cudaSetDevice(b->device);
+  auto bail = [&](cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e);
+    sgnb_batch_destroy(b);
+    return bfail(nullptr, e == cudaErrorMemoryAllocation ? SGNB_ERR_NOMEM : SGNB_ERR_CUDA, m);
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evRead, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->dconsts, n * sizeof(RhsConsts));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dargs, n * sizeof(StageArgs));
+  if (e == cudaSuccess) e = cudaMallocHost(&b->hargs, n * sizeof(StageArgs));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dctrl, n * sizeof(CtrlState));
+  if (e == cudaSuccess) e = cudaMallocHost(&b->hctrl, n * sizeof(CtrlState));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dpart, n * sizeof(double*));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dntot, n * sizeof(long long));
+  if (e != cudaSuccess) return bail(e, "batch buffers");
+  std::vector<RhsConsts> hc(n);
+  std::vector<long long> ht(n);
+  for (int i = 0; i < n; ++i) {
+    hc[i] = b->ctx[i]->C;
+    ht[i] = b->ctx[i]->ntot;
+  }
+  e = cudaMemcpy(b->dconsts, hc.data(), n * sizeof(RhsConsts), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->dntot, ht.data(), n * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return bail(e, "batch upload");
+  std::vector<long long> maxTiles(n, 0);
+  // work lists per tile shape: instance-major tiles (8x4 tiles also fix the per-instance
+  // partial count, which the controllers reduce; other shapes have more or fewer tiles)
+  for (int sh = 0; sh < 3; ++sh) {
+    const int tx = dev::batch_tile_tx(sh), ty = 32 / tx;
+    std::vector<int> inst;
+    std::vector<long long> start(n + 1, 0);
+    std::vector<int> nb(n);
+    for (int i = 0; i < n; ++i) {
+      const long long nt = (long long)((b->ctx[i]->desc.Nx + tx - 1) / tx) *
+                           ((b->ctx[i]->desc.Ny + ty - 1) / ty);
+      start[i + 1] = start[i] + nt;
+      inst.insert(inst.end(), (size_t)nt, i);
+      nb[i] = (int)nt;
+      if (nt > maxTiles[i]) maxTiles[i] = nt;
+    }
+    b->ntiles[sh] = start[n];
+    e = cudaMalloc(&b->dnblk[sh], n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(b->dnblk[sh], nb.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dtile_inst[sh], inst.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->dtile_start[sh], (n + 1) * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMemcpy(b->dtile_inst[sh], inst.data(), inst.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->dtile_start[sh], start.data(), (n + 1) * sizeof(long long), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return bail(e, "batch work list");
+  }
+  long long totPart = 0;
+  for (int i = 0; i < n; ++i) totPart += 3 * maxTiles[i];
+  e = cudaMalloc(&b->dpartbuf, totPart * sizeof(double));
+  if (e != cudaSuccess) return bail(e, "batch partials");
+  b->hpart.resize(n);
+  for (long long i = 0, off = 0; i < n; off += 3 * maxTiles[i], ++i) b->hpart[i] = b->dpartbuf + off;
+  e = cudaMemcpy(b->dpart, b->hpart.data(), n * sizeof(double*), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return bail(e, "batch partials");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  b->shape = 0;
+  b->blocks = 2 * sms;
+  *out = b;
+  return SGNB_OK;
+}
+
+int sgnb_batch_destroy(sgnb_batch* b) {
+  if (!b) return SGNB_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->chunk) cudaGraphExecDestroy(b->chunk);
+  if (b->evRead) cudaEventDestroy(b->evRead);
+  cudaFree(b->dconsts); cudaFree(b->dargs); cudaFree(b->dctrl); cudaFree(b->dpart);
+  cudaFree(b->dntot); cudaFree(b->dpartbuf);
+  if (b->hargs) cudaFreeHost(b->hargs);
+  if (b->hctrl) cudaFreeHost(b->hctrl);
+  for (int sh = 0; sh < 3; ++sh) {
+    cudaFree(b->dtile_inst[sh]); cudaFree(b->dtile_start[sh]); cudaFree(b->dnblk[sh]);
+  }
+  if (b->stream) cudaStreamDestroy(b->stream);
+  for (sgnb_ctx* c : b->ctx) sgnb_destroy(c);
+  delete b;
+  return SGNB_OK;
+}
+
+int sgnb_batch_size(const sgnb_batch* b) { return b ? b->n : 0; }
+
+sgnb_ctx* sgnb_batch_instance(sgnb_batch* b, int i) {
+  return (b && i >= 0 && i < b->n) ? b->ctx[i] : nullptr;
+}
+
+int sgnb_batch_set_config(sgnb_batch* b, int shape, int blocks) {
+  if (!b || shape < 0 || shape > 2 || blocks < 1) return bfail(b, SGNB_ERR_INVALID, "shape 0..2, blocks >= 1");
+  b->shape = shape;
+  b->blocks = blocks;
+  return SGNB_OK;
+}
+
+int sgnb_batch_get_config(const sgnb_batch* b, int* shape, int* blocks) {
+  if (!b) return SGNB_ERR_INVALID;
+  if (shape) *shape = b->shape;
+  if (blocks) *blocks = b->blocks;
+  return SGNB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int batch_init_ctrls(sgnb_batch* b, const double* dt0, long long nsteps, const sgnb_rk_opts& o) {
+  for (int i = 0; i < b->n; ++i) {
+    CtrlState& h = b->hctrl[i];
+    init_ctrl(b->ctx[i], h, o);
+    h.log = nullptr;
+    h.t = 0.0;
+    h.tEnd = 1e300;
+    h.dt = (o.dtMax < dt0[i]) ? o.dtMax : dt0[i];
+    h.errPrev = 1.0;
+    h.cur = b->ctx[i]->cur;
+    h.rhsEvals = 1;
+    h.maxAccepted = nsteps;
+  }
+  // the instances' own uploads ran on their context streams
+  for (sgnb_ctx* c : b->ctx) SGNB_BCU(b, cudaStreamSynchronize(c->stream));
+  return SGNB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sgnb_batch_integrate_steps(sgnb_batch* b, const double* dt0, long long nsteps,
+                               const sgnb_rk_opts* opts, sgnb_rk_stats* stats) {
+  if (!b || !dt0 || nsteps < 1) return bfail(b, SGNB_ERR_INVALID, "dt0, nsteps >= 1");
+  SGNB_BCU(b, cudaSetDevice(b->device));
+  sgnb_rk_opts o;
+  if (opts) o = *opts; else sgnb_rk_opts_init(&o);
+  if (int rc = batch_init_ctrls(b, dt0, nsteps, o)) return rc;
+  if (int rc = batch_run(b)) return rc;
+  int status = SGNB_OK;
+  for (int i = 0; i < b->n; ++i) {
+    const CtrlState& h = b->hctrl[i];
+    if (stats) {
+      sgnb_rk_stats& st = stats[i];
+      st.accepted = h.accepted; st.rejected = h.rejected; st.rhsEvals = h.rhsEvals;
+      st.attempts = h.attempts; st.tReached = h.tReached; st.dtLast = h.dtLast;
+      st.maxNormLast = h.maxNormLast;
+      st.aborted = h.done == 2 ? 1 : (h.done == 3 ? 2 : 0);
+      st.status = h.done == 3 ? SGNB_ERR_NAN : SGNB_OK;
+      st.kernel_launches = b->launches;
+    }
+    if (h.done == 3) status = SGNB_ERR_NAN;
+  }
+  if (status) return bfail(b, status, "non-finite error estimate in an instance");
+  return SGNB_OK;
+}
+
+int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_out) {
+  if (!b || !dt0 || reps < 1) return bfail(b, SGNB_ERR_INVALID, "dt0, reps >= 1");
+  SGNB_BCU(b, cudaSetDevice(b->device));
+  sgnb_rk_opts o;
+  sgnb_rk_opts_init(&o);
+  // One attempt's three stage launches per repetition. Without the controller the
+  // ping-pong index never flips, so the state the instances hold is left as it was:
+  // the launches only write k2, k3, the other state buffer and the error partials.
+  if (int rc = batch_init_ctrls(b, dt0, 1, o)) return rc;
+  if (int rc = batch_prepare(b)) return rc;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  cudaEvent_t e0, e1;
+  SGNB_BCU(b, cudaEventCreate(&e0));
+  SGNB_BCU(b, cudaEventCreate(&e1));
+  double best = 1e300;
+  int bestShape = 0, bestBlocks = 2 * sms;
+  int rc = SGNB_OK;
+  for (int sh = 0; sh < 3 && rc == SGNB_OK; ++sh) {
+    for (int f = 1; f <= kTuneFactors && rc == SGNB_OK; ++f) {
+      const int blocks = f * sms;
+      auto run = [&](int count) {
+        cudaError_t e = cudaSuccess;
+        for (int r = 0; r < count && e == cudaSuccess; ++r) {
+          e = dev::launch_fused_batch(1, sh, blocks, batch_args(b, sh, 0, 0.5), b->stream);
+          if (e == cudaSuccess)
+            e = dev::launch_fused_batch(1, sh, blocks, batch_args(b, sh, 1, 0.75), b->stream);
+          if (e == cudaSuccess)
+            e = dev::launch_fused_batch(2, sh, blocks, batch_args(b, sh, 0, 0.0), b->stream);
+        }
+        return e;
+      };
+      cudaError_t e = run(1);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+      if (e == cudaSuccess) e = run(reps);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) { rc = bfail(b, SGNB_ERR_CUDA, std::string("autotune: ") + cudaGetErrorName(e)); break; }
+      const double per = (double)ms / reps;
+      if (ms_out) ms_out[sh * kTuneFactors + (f - 1)] = per;
+      if (per < best) { best = per; bestShape = sh; bestBlocks = blocks; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->shape = bestShape;
+  b->blocks = bestBlocks;
+  return SGNB_OK;
+}
+
+const char* sgnb_batch_last_error(const sgnb_batch* b) {
+  return b ? b->err.c_str() : g_create_error.c_str();
 }
 
 }  // extern "C"

@@ -79,6 +79,23 @@ struct StageArgsM {
   double* partials;
 };
 
+// Work list of a batched launch: tile t belongs to instance tile_inst[t] and is that
+// instance's local tile t - tile_start[inst]; per-instance constants and buffers.
+struct FrTablesDev {
+  double D[25], gLp[5], gRp[5];
+};
+
+struct BatchArgs {
+  FrTablesDev tables;   // shared by every instance (P = 4 GLL)
+  const RhsConsts* consts;
+  const StageArgs* args;
+  const int* tile_inst;
+  const long long* tile_start;
+  long long ntiles;
+  int kin_k2;
+  double coef;
+};
+
 namespace dev {
 // Launchers (one translation unit per arithmetic mode).
 cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
@@ -91,6 +108,15 @@ cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A
                                cudaStream_t s);
 cudaError_t prepare_fused_mixed();
 int fused_grid_blocks(int Nx, int Ny);
+// Batched launch (FP64 fast): tile shape shape_id (0: 8x4, 1: 16x2, 2: 4x8), grid of
+// `blocks` persistent CTAs.
+cudaError_t launch_fused_batch(int mode, int shape_id, int blocks, const BatchArgs& B,
+                               cudaStream_t s);
+cudaError_t prepare_fused_batch();
+int batch_tile_tx(int shape_id);
+cudaError_t launch_controller_batch(CtrlState* ctrls, const double* const* partials,
+                                    const int* nblk, const long long* n, int ninst,
+                                    cudaStream_t s);
 size_t fused_smem_bytes();
 
 // Controller of one adaptive attempt: deterministic reduction of the per-CTA error

@@ -44,13 +44,11 @@ namespace dev {
 constexpr int NP = 5;          // GLL points per direction (P = 4)
 constexpr int NPP = 25;        // nodes per element
 constexpr int NV = 5;          // conserved fields h, hu, hv, hw, hp
-constexpr int TX = 8;          // tile width in elements
-constexpr int TY = 4;          // tile height in elements
-constexpr int TE = TX * TY;    // elements per tile = lanes per warp
+constexpr int TE = 32;         // elements per tile = lanes per warp
 constexpr int NWARP = 5;       // one warp per GLL line index
 constexpr int NTHR = 32 * NWARP;
-
-static_assert(TE == 32, "one tile element per lane");
+constexpr int NIT = TE * NPP / NTHR;                   // own-node items per thread
+static_assert(TE * NPP == NIT * NTHR, "own nodes split evenly over the threads");
 
 // Stage modes of the fused kernel.
 enum : int {
@@ -59,40 +57,42 @@ enum : int {
   MODE_FSAL = 2    // uNew = u + dt(2/9 k1 + 1/3 k2 + 4/9 k3); k4 = R(uNew); error partials
 };
 
-struct Smem {
-  double U[NV][TE][NPP];       // tile state (input of R)
-  double H[TE][NPP];           // nodal still depth
-  double Hx[TE][NPP];          // nodal dH/dx
-  double Hy[TE][NPP];          // nodal dH/dy
-  double G[NV + 1][TE][NPP];   // column-pass results dG (5 fields) and By; then dU
-  // halo node states, flat index q = t + NP * (slot + NHALO * v):
-  //   slot 0..TY-1        node (4,t) of the element left of tile row slot
-  //   slot TY..2TY-1      node (0,t) of the element right of tile row slot-TY
-  //   slot 2TY..2TY+TX-1  node (t,4) of the element below tile column slot-2TY
-  //   slot 2TY+TX..       node (t,0) of the element above tile column slot-2TY-TX
-  double halo[NV * (2 * TY + 2 * TX) * NP];
-  // face depths, flat: HfX[TE][NP] (left edges), HfY[TE][NP] (bottom edges),
-  // HfXR[TY][NP] (right edge of the last tile column), HfYT[TX][NP] (top edge of the
-  // last tile row)
-  double Hf[(2 * TE + TY + TX) * NP];
-  double red[NWARP][3];        // block reduction of the error partials
+// A tile of TX x TY = 32 elements (TX in 4, 8, 16) and its shared-memory layout.
+template <int TX_, int TY_>
+struct Tile {
+  static constexpr int TX = TX_, TY = TY_;
+  static_assert(TX * TY == TE, "one tile element per lane");
+  static constexpr int NHALO = 2 * TY + 2 * TX;                 // halo slots per field
+  static constexpr int RUN = TX * NPP;                          // doubles per tile row and field
+  static constexpr int NHIT = (NV * NHALO * NP + NTHR - 1) / NTHR;  // halo items per thread
+  static constexpr int NFACE = (2 * TE + TY + TX) * NP;
+  static constexpr int NFIT = (NFACE + NTHR - 1) / NTHR;        // face-depth items per thread
+  struct Smem {
+    double U[NV][TE][NPP];       // tile state (input of R)
+    double H[TE][NPP];           // nodal still depth
+    double Hx[TE][NPP];          // nodal dH/dx
+    double Hy[TE][NPP];          // nodal dH/dy
+    double G[NV + 1][TE][NPP];   // column-pass results dG (5 fields) and By; then dU
+    // halo node states, flat index q = t + NP * (slot + NHALO * v):
+    //   slot 0..TY-1        node (4,t) of the element left of tile row slot
+    //   slot TY..2TY-1      node (0,t) of the element right of tile row slot-TY
+    //   slot 2TY..2TY+TX-1  node (t,4) of the element below tile column slot-2TY
+    //   slot 2TY+TX..       node (t,0) of the element above tile column slot-2TY-TX
+    double halo[NV * NHALO * NP];
+    // face depths, flat: HfX[TE][NP] (left edges), HfY[TE][NP] (bottom edges),
+    // HfXR[TY][NP] (right edge of the last tile column), HfYT[TX][NP] (top edge of the
+    // last tile row)
+    double Hf[NFACE];
+    double red[NWARP][3];        // block reduction of the error partials
+  };
+  static __device__ __forceinline__ double& hf_x(Smem& S, int i, int t) { return S.Hf[i * NP + t]; }
+  static __device__ __forceinline__ double& hf_y(Smem& S, int i, int t) { return S.Hf[(TE + i) * NP + t]; }
+  static __device__ __forceinline__ double& hf_xr(Smem& S, int iy, int t) { return S.Hf[(2 * TE + iy) * NP + t]; }
+  static __device__ __forceinline__ double& hf_yt(Smem& S, int ix, int t) { return S.Hf[(2 * TE + TY + ix) * NP + t]; }
+  static __device__ __forceinline__ double& halo_at(Smem& S, int v, int slot, int t) {
+    return S.halo[t + NP * (slot + NHALO * v)];
+  }
 };
-
-constexpr int NHALO = 2 * TY + 2 * TX;                 // halo slots per field
-constexpr int RUN = TX * NPP;                          // doubles per tile row and field
-constexpr int NIT = TY * RUN / NTHR;                   // own-node items per thread
-static_assert(TY * RUN == NIT * NTHR, "own nodes split evenly over the threads");
-constexpr int NHIT = (NV * NHALO * NP + NTHR - 1) / NTHR;          // halo items per thread
-constexpr int NFACE = (2 * TE + TY + TX) * NP;
-constexpr int NFIT = (NFACE + NTHR - 1) / NTHR;                    // face-depth items
-
-__device__ __forceinline__ double& hf_x(Smem& S, int i, int t) { return S.Hf[i * NP + t]; }
-__device__ __forceinline__ double& hf_y(Smem& S, int i, int t) { return S.Hf[(TE + i) * NP + t]; }
-__device__ __forceinline__ double& hf_xr(Smem& S, int iy, int t) { return S.Hf[(2 * TE + iy) * NP + t]; }
-__device__ __forceinline__ double& hf_yt(Smem& S, int ix, int t) { return S.Hf[(2 * TE + TY + ix) * NP + t]; }
-__device__ __forceinline__ double& halo_at(Smem& S, int v, int slot, int t) {
-  return S.halo[t + NP * (slot + NHALO * v)];
-}
 
 // Asynchronous global -> shared copy of one double (cp.async, no register staging), and
 // the wait for all of this thread's outstanding copies.
@@ -246,8 +246,8 @@ __device__ __forceinline__ double flux_field(const RhsConsts& C, int v, double h
 // derivative of node m, then emit(m, v, d, q) with the FR-corrected derivative of flux
 // field v at node m (both already divided by J). The flux of each field is rebuilt from
 // per-node quantities inside the contraction, which keeps the live set small.
-template <bool EXACT, int DIR, class EmitH, class Emit>
-__device__ __forceinline__ void line_pass(const RhsConsts& C, const double (&Un)[NP][NV],
+template <bool EXACT, int DIR, class TB, class EmitH, class Emit>
+__device__ __forceinline__ void line_pass(const RhsConsts& C, const TB& Tb, const double (&Un)[NP][NV],
                                           const double (&Hn)[NP], const double* nLo,
                                           const double* nHi, double HfLo, double HfHi,
                                           EmitH&& emit_dh, Emit&& emit) {
@@ -311,14 +311,14 @@ __device__ __forceinline__ void line_pass(const RhsConsts& C, const double (&Un)
       if constexpr (EXACT) {
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) s += C.D[m * NP + k] * Un[k][0];
-        s += jhLo * C.gLp[m] + jhHi * C.gRp[m];
+        for (int k = 0; k < NP; ++k) s += Tb.D[m * NP + k] * Un[k][0];
+        s += jhLo * Tb.gLp[m] + jhHi * Tb.gRp[m];
         dh = s / (DIR == 0 ? C.Jx : C.Jy);
       } else {
-        double s = jhLo * C.gLp[m];
-        s = fma(jhHi, C.gRp[m], s);
+        double s = jhLo * Tb.gLp[m];
+        s = fma(jhHi, Tb.gRp[m], s);
 #pragma unroll
-        for (int k = 0; k < NP; ++k) s = fma(C.D[m * NP + k], Un[k][0], s);
+        for (int k = 0; k < NP; ++k) s = fma(Tb.D[m * NP + k], Un[k][0], s);
         dh = s * (DIR == 0 ? C.iJx : C.iJy);
       }
       emit_dh(m, dh, q[m]);
@@ -336,15 +336,15 @@ __device__ __forceinline__ void line_pass(const RhsConsts& C, const double (&Un)
       if constexpr (EXACT) {
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < NP; ++k) s += C.D[m * NP + k] * F[k];
-        const double c = jLo[v] * C.gLp[m] + jHi[v] * C.gRp[m];
+        for (int k = 0; k < NP; ++k) s += Tb.D[m * NP + k] * F[k];
+        const double c = jLo[v] * Tb.gLp[m] + jHi[v] * Tb.gRp[m];
         d = (s + c) / (DIR == 0 ? C.Jx : C.Jy);
       } else {
         // accumulate with the unscaled tables, one rounding for 1/J at the end
-        double s = jLo[v] * C.gLp[m];
-        s = fma(jHi[v], C.gRp[m], s);
+        double s = jLo[v] * Tb.gLp[m];
+        s = fma(jHi[v], Tb.gRp[m], s);
 #pragma unroll
-        for (int k = 0; k < NP; ++k) s = fma(C.D[m * NP + k], F[k], s);
+        for (int k = 0; k < NP; ++k) s = fma(Tb.D[m * NP + k], F[k], s);
         d = s * (DIR == 0 ? C.iJx : C.iJy);
       }
       emit(m, v, d, q[m]);
@@ -360,10 +360,16 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
   ghost[DIR == 0 ? 1 : 2] = -own[DIR == 0 ? 1 : 2];
 }
 
-template <int MODE, bool EXACT>
-__global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const StageArgs A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+// One tile of the fused right-hand side / stage kernel: tile (bx, by) of the mesh whose
+// constants are C, error partial slot blk. Shared by the single-instance kernel and the
+// batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
+template <int MODE, bool EXACT, int TX_, int TY_, class TB>
+__device__ __forceinline__ void fused_tile(const RhsConsts& C, const TB& Tb, const StageArgs& A,
+                                           int bx, int by, long long blk,
+                                           typename Tile<TX_, TY_>::Smem& S) {
+  using T = Tile<TX_, TY_>;
+  constexpr int TX = T::TX, TY = T::TY, NHALO = T::NHALO, RUN = T::RUN;
+  constexpr int NHIT = T::NHIT, NFACE = T::NFACE, NFIT = T::NFIT;
 
   // ---- controller state (stage modes only) ---------------------------------
   int cur = 0;
@@ -390,7 +396,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
   const int warp = tid >> 5, lane = tid & 31;
   const int Nx = C.Nx, Ny = C.Ny;
   const long long Nd = C.Nd;
-  const int ex0 = blockIdx.x * TX, ey0 = blockIdx.y * TY;
+  const int ex0 = bx * TX, ey0 = by * TY;
   const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
   const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
   const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
@@ -590,7 +596,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<1>(Un[0], nLo);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nLo[v] = halo_at(S, v, 2 * TY + ix, j);
+      for (int v = 0; v < NV; ++v) nLo[v] = T::halo_at(S, v, 2 * TY + ix, j);
     }
     if (iy + 1 < TYv) {
 #pragma unroll
@@ -599,12 +605,12 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<1>(Un[NP - 1], nHi);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nHi[v] = halo_at(S, v, 2 * TY + TX + ix, j);
+      for (int v = 0; v < NV; ++v) nHi[v] = T::halo_at(S, v, 2 * TY + TX + ix, j);
     }
-    const double HfLo = hf_y(S, i, j);
-    const double HfHi = (iy + 1 < TYv) ? hf_y(S, i + TX, j) : hf_yt(S, ix, j);
+    const double HfLo = T::hf_y(S, i, j);
+    const double HfHi = (iy + 1 < TYv) ? T::hf_y(S, i + TX, j) : T::hf_yt(S, ix, j);
     line_pass<EXACT, 1>(
-        C, Un, Hn, nLo, nHi, HfLo, HfHi,
+        C, Tb, Un, Hn, nLo, nHi, HfLo, HfHi,
         [&](int b, double dh, const Prim<EXACT>& q) {
           S.G[NV][i][j + NP * b] = C.mc2 * q.v * dh;  // ncpY (sgn_flux2d.h:156-161)
         },
@@ -631,7 +637,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<0>(Un[0], nLo);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nLo[v] = halo_at(S, v, iy, j);
+      for (int v = 0; v < NV; ++v) nLo[v] = T::halo_at(S, v, iy, j);
     }
     if (ix + 1 < TXv) {
 #pragma unroll
@@ -640,13 +646,13 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
       mirror<0>(Un[NP - 1], nHi);
     } else {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nHi[v] = halo_at(S, v, TY + iy, j);
+      for (int v = 0; v < NV; ++v) nHi[v] = T::halo_at(S, v, TY + iy, j);
     }
-    const double HfLo = hf_x(S, i, j);
-    const double HfHi = (ix + 1 < TXv) ? hf_x(S, i + 1, j) : hf_xr(S, iy, j);
+    const double HfLo = T::hf_x(S, i, j);
+    const double HfHi = (ix + 1 < TXv) ? T::hf_x(S, i + 1, j) : T::hf_xr(S, iy, j);
     double dhx[NP];
     line_pass<EXACT, 0>(
-        C, Un, Hn, nLo, nHi, HfLo, HfHi,
+        C, Tb, Un, Hn, nLo, nHi, HfLo, HfHi,
         [&](int a, double dh, const Prim<EXACT>&) { dhx[a] = dh; },
         [&](int a, int v, double d, const Prim<EXACT>& q) {
           const int loc = a + NP * j;
@@ -772,11 +778,57 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
         m = m < S.red[w][1] ? S.red[w][1] : m;
         n += S.red[w][2];
       }
-      const long long blk = (long long)blockIdx.y * gridDim.x + blockIdx.x;
       A.partials[3 * blk + 0] = s;
       A.partials[3 * blk + 1] = m;
       A.partials[3 * blk + 2] = n;
     }
+  }
+}
+
+
+template <int MODE, bool EXACT>
+__global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const StageArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  using T = Tile<8, 4>;
+  T::Smem& S = *reinterpret_cast<T::Smem*>(smem_raw);
+  fused_tile<MODE, EXACT, 8, 4>(C, C, A, blockIdx.x, blockIdx.y,
+                                (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
+}
+
+// Batched form: one persistent launch walks the tiles of many independent instances
+// (the work list tile_inst / tile_start), each with its own constants, buffers and
+// controller. The instance's constants and buffer pointers are copied into shared
+// memory once per tile.
+template <int MODE, bool EXACT, int TX_, int TY_>
+__global__ void __launch_bounds__(NTHR, 2) k_fused_batch(const BatchArgs B) {
+  // FR tables come from the kernel parameters (constant bank): the same for every
+  // instance (P = 4 GLL)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  using T = Tile<TX_, TY_>;
+  typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
+  __shared__ RhsConsts Cs;
+  __shared__ StageArgs As;
+  for (long long t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+    const int inst = B.tile_inst[t];
+    const long long lt = t - B.tile_start[inst];
+    __syncthreads();  // the previous tile is done with Cs / As
+    {
+      const unsigned* src = reinterpret_cast<const unsigned*>(B.consts + inst);
+      unsigned* dst = reinterpret_cast<unsigned*>(&Cs);
+      for (int w = threadIdx.x; w < (int)(sizeof(RhsConsts) / 4); w += NTHR) dst[w] = src[w];
+      const unsigned* srca = reinterpret_cast<const unsigned*>(B.args + inst);
+      unsigned* dsta = reinterpret_cast<unsigned*>(&As);
+      for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 4); w += NTHR) dsta[w] = srca[w];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      As.kin_k2 = B.kin_k2;
+      As.coef = B.coef;
+      if (MODE == MODE_STAGE) As.out = B.kin_k2 ? As.K3 : As.K2;
+    }
+    __syncthreads();
+    const int ntx = (Cs.Nx + TX_ - 1) / TX_;
+    fused_tile<MODE, EXACT, TX_, TY_>(Cs, B.tables, As, (int)(lt % ntx), (int)(lt / ntx), lt, S);
   }
 }
 

@@ -10,7 +10,7 @@ cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
   return launch_any(mode, C, A, s);
 }
 cudaError_t prepare_fused_exact() { return prepare_all(); }
-int fused_grid_blocks(int Nx, int Ny) { return ((Nx + TX - 1) / TX) * ((Ny + TY - 1) / TY); }
-size_t fused_smem_bytes() { return sizeof(Smem); }
+int fused_grid_blocks(int Nx, int Ny) { return ((Nx + 7) / 8) * ((Ny + 3) / 4); }
+size_t fused_smem_bytes() { return sizeof(Tile<8, 4>::Smem); }
 }  // namespace dev
 }  // namespace sgnb

@@ -10,5 +10,54 @@ cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A, 
   return launch_any(mode, C, A, s);
 }
 cudaError_t prepare_fused_fast() { return prepare_all(); }
+
+template <int MODE, int TXs, int TYs>
+static cudaError_t launch_b(int blocks, const BatchArgs& B, cudaStream_t s) {
+  k_fused_batch<MODE, false, TXs, TYs><<<blocks, NTHR, sizeof(typename Tile<TXs, TYs>::Smem), s>>>(B);
+  return cudaGetLastError();
+}
+
+template <int TXs, int TYs>
+static cudaError_t launch_shape(int mode, int blocks, const BatchArgs& B, cudaStream_t s) {
+  switch (mode) {
+    case MODE_RHS: return launch_b<MODE_RHS, TXs, TYs>(blocks, B, s);
+    case MODE_STAGE: return launch_b<MODE_STAGE, TXs, TYs>(blocks, B, s);
+    case MODE_FSAL: return launch_b<MODE_FSAL, TXs, TYs>(blocks, B, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_fused_batch(int mode, int shape_id, int blocks, const BatchArgs& B,
+                               cudaStream_t s) {
+  switch (shape_id) {
+    case 0: return launch_shape<8, 4>(mode, blocks, B, s);
+    case 1: return launch_shape<16, 2>(mode, blocks, B, s);
+    case 2: return launch_shape<4, 8>(mode, blocks, B, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int batch_tile_tx(int shape_id) { return shape_id == 1 ? 16 : (shape_id == 2 ? 4 : 8); }
+
+template <int TXs, int TYs>
+static cudaError_t prepare_shape() {
+  const int bytes = (int)sizeof(typename Tile<TXs, TYs>::Smem);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_fused_batch<MODE_RHS, false, TXs, TYs>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(k_fused_batch<MODE_STAGE, false, TXs, TYs>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(k_fused_batch<MODE_FSAL, false, TXs, TYs>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t prepare_fused_batch() {
+  cudaError_t e = prepare_shape<8, 4>();
+  if (e == cudaSuccess) e = prepare_shape<16, 2>();
+  if (e == cudaSuccess) e = prepare_shape<4, 8>();
+  return e;
+}
 }  // namespace dev
 }  // namespace sgnb

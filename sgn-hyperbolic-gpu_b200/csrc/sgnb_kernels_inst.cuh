@@ -10,13 +10,13 @@ namespace dev {
 
 template <int MODE>
 static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
-  const dim3 grid((C.Nx + TX - 1) / TX, (C.Ny + TY - 1) / TY);
-  k_fused<MODE, SGNB_EXACT><<<grid, NTHR, sizeof(Smem), s>>>(C, A);
+  const dim3 grid((C.Nx + 7) / 8, (C.Ny + 3) / 4);
+  k_fused<MODE, SGNB_EXACT><<<grid, NTHR, sizeof(Tile<8, 4>::Smem), s>>>(C, A);
   return cudaGetLastError();
 }
 
 static cudaError_t prepare_all() {
-  const int bytes = (int)sizeof(Smem);
+  const int bytes = (int)sizeof(Tile<8, 4>::Smem);
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)

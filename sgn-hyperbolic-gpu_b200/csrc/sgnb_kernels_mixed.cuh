@@ -282,8 +282,17 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
                          "l"(I.k + (long long)v * Nd + gof[u]) : "memory");
           }
-      cp_async_wait_all();
     }
+    // stage mode: every u load of the tile in flight before the first combination
+    double ux[NV][NIT];
+    if constexpr (MODE == MODE_STAGE) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) ux[v][u] = I.u[(long long)v * Nd + gof[u]];
+    }
+    if constexpr (MODE == MODE_STAGE) cp_async_wait_all();  // k and the statics have landed
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       double x[NIT];
@@ -291,7 +300,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           if constexpr (MODE == MODE_STAGE)
-            x[u] = I.u[(long long)v * Nd + gof[u]] + I.acoef * (double)(&S.G[v][0][0])[sof[u]];
+            x[u] = ux[v][u] + I.acoef * (double)(&S.G[v][0][0])[sof[u]];
           else
             x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
         }

@@ -20,8 +20,8 @@ __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b 
 // accept if the RMS scaled error <= 1 (rk.cpp:129-142), PI update clamped to
 // [facMin, facMax] (:148-152), dtMin abort (:155-160), and the loop test and the
 // end-time clip of the next attempt (:95-97).
-__global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const double* partials,
-                                                             int nblk, long long n) {
+__device__ __forceinline__ void controller_block(CtrlState* c, const double* partials, int nblk,
+                                                 long long n) {
   __shared__ double ss[kCtrlThreads], sm[kCtrlThreads], sn[kCtrlThreads];
   if (c->done) return;
   const int t = threadIdx.x;
@@ -100,6 +100,19 @@ __global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const
   if (c->t + c->dt > tEnd) c->dt = tEnd - c->t;
 }
 
+__global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const double* partials,
+                                                             int nblk, long long n) {
+  controller_block(c, partials, nblk, n);
+}
+
+// Batched controller: block i runs instance i's controller on its own partials.
+__global__ void __launch_bounds__(kCtrlThreads) k_controller_batch(CtrlState* ctrls,
+                                                                   const double* const* partials,
+                                                                   const int* nblk, const long long* n) {
+  const int i = blockIdx.x;
+  controller_block(ctrls + i, partials[i], nblk[i], n[i]);
+}
+
 struct QW {
   double w[5];
 };
@@ -148,6 +161,13 @@ __global__ void __launch_bounds__(256) k_diag(int what, const RhsConsts C, const
 cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk, long long n,
                               cudaStream_t s) {
   k_controller<<<1, kCtrlThreads, 0, s>>>(c, partials, nblk, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_controller_batch(CtrlState* ctrls, const double* const* partials,
+                                    const int* nblk, const long long* n, int ninst,
+                                    cudaStream_t s) {
+  k_controller_batch<<<ninst, kCtrlThreads, 0, s>>>(ctrls, partials, nblk, n);
   return cudaGetLastError();
 }
 

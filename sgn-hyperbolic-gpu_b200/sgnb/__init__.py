@@ -140,6 +140,16 @@ SIGNATURES = {
                                         C.POINTER(C.c_void_p)]),
     "sgnb_fr_tables": (C.c_int, [C.c_int] + [_dp] * 7),
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
+    "sgnb_batch_create": (C.c_int, [C.POINTER(_Desc), C.c_int, C.POINTER(C.c_void_p)]),
+    "sgnb_batch_destroy": (C.c_int, [C.c_void_p]),
+    "sgnb_batch_size": (C.c_int, [C.c_void_p]),
+    "sgnb_batch_instance": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "sgnb_batch_integrate_steps": (C.c_int, [C.c_void_p, _dp, C.c_longlong, C.POINTER(_Opts),
+                                             C.POINTER(_Stats)]),
+    "sgnb_batch_set_config": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "sgnb_batch_get_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "sgnb_batch_autotune": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp]),
+    "sgnb_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "sgnb_status_string": (C.c_char_p, [C.c_int]),
     "sgnb_last_error": (C.c_char_p, [C.c_void_p]),
 }
@@ -231,6 +241,14 @@ def setup_bathymetry(P=4, Nx=8, Ny=6, Lx=10.0, Ly=8.0, bathy_kind=BATHY_NONE, ba
     return out
 
 
+class _DeviceArray:
+    """A raw device pointer exposed through __cuda_array_interface__ (float64, 1-D)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = dict(shape=(n,), typestr="<f8", data=(ptr, False),
+                                             version=3, strides=None)
+
+
 class SGN2DB200:
     """Device solver with the interface of sgn::SGN2DCuda / sgn::SGN2D.
 
@@ -244,22 +262,27 @@ class SGN2DB200:
     def __init__(self, P=4, Nx=8, Ny=6, Lx=10.0, Ly=8.0, g=9.81, c=0.0, gamma=1.5,
                  nManning=0.0, bc_x=BC_PERIODIC, bc_y=BC_PERIODIC, precision=FP64_EXACT,
                  device=0, bathy_kind=BATHY_NONE, bathy_par=(), tables=None,
-                 bathy_arrays=None):
+                 bathy_arrays=None, _handle=None):
         self._h = None
-        holder = _DescHolder(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y, precision,
-                             device, bathy_kind, bathy_par, tables, bathy_arrays)
-        h = C.c_void_p()
-        _check(lib().sgnb_create(C.byref(holder.desc), C.byref(h)))
+        self._owned = _handle is None
+        if _handle is None:
+            holder = _DescHolder(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y,
+                                 precision, device, bathy_kind, bathy_par, tables, bathy_arrays)
+            h = C.c_void_p()
+            _check(lib().sgnb_create(C.byref(holder.desc), C.byref(h)))
+        else:
+            h = C.c_void_p(_handle)
         self._h = h
         self.P, self.Nx, self.Ny, self.Lx, self.Ly = P, Nx, Ny, Lx, Ly
         self.Nd = int(lib().sgnb_ndof(h))
         self.n = 5 * self.Nd
         self.precision = precision
+        self.device = device
 
     def close(self):
-        if self._h:
+        if self._h and self._owned:
             lib().sgnb_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -336,6 +359,25 @@ class SGN2DB200:
         _check(lib().sgnb_state_device_ptr(self._h, C.byref(u), C.byref(s)), self._h)
         return u.value, s.value
 
+    def state_tensor(self):
+        """The current device state as a float64 torch tensor view (no copy). Valid until
+        the next integration (which may switch the state buffer); the library works on its
+        own stream, so synchronise before reading or writing it from torch."""
+        import torch
+
+        u, _ = self.state_device_ptr()
+        return torch.as_tensor(_DeviceArray(u, self.n), device=f"cuda:{self.device}")
+
+    def upload_tensor(self, t):
+        """Device-to-device upload of a float64 torch tensor holding a state."""
+        import torch
+
+        if t.dtype != torch.float64 or t.numel() != self.n:
+            raise ValueError("SGN2DB200.upload_tensor: float64 tensor of size 5 * nDof expected")
+        torch.cuda.synchronize(self.device)
+        self.state_tensor().copy_(t.reshape(-1))
+        torch.cuda.synchronize(self.device)
+
     # --- integrators -------------------------------------------------------------
     def integrate_adaptive(self, t0, tEnd, dt0, opt: AdaptiveRKOptions | None = None,
                            raise_on_nan=True) -> AdaptiveRKStats:
@@ -394,3 +436,107 @@ class SGN2DB200:
 
     def energy(self):
         return self._scalar(lib().sgnb_energy)
+
+
+def _stats(st) -> AdaptiveRKStats:
+    return AdaptiveRKStats(st.accepted, st.rejected, st.rhsEvals, st.attempts, st.tReached,
+                           st.dtLast, st.maxNormLast, st.aborted, st.kernel_launches)
+
+
+class SGNBatch:
+    """Many independent SGN2D instances advanced together (FP64_FAST).
+
+    ``instances`` is a list of keyword dicts for SGN2DB200 (mesh size, domain, c, gamma,
+    boundaries, bathymetry). Every RK stage is one persistent launch over the tiles of all
+    instances; each instance keeps its own adaptive controller. ``self[i]`` is a view of
+    instance i with the single-instance methods (upload, download, rhs, mass, ...).
+    """
+
+    def __init__(self, instances, device=0):
+        self._b = None
+        holders = []
+        for kw in instances:
+            kw = dict(kw)
+            kw.setdefault("precision", FP64_FAST)
+            kw["device"] = device
+            args = [kw.pop(k, dflt) for k, dflt in (
+                ("P", 4), ("Nx", 8), ("Ny", 6), ("Lx", 10.0), ("Ly", 8.0), ("g", 9.81),
+                ("c", 0.0), ("gamma", 1.5), ("nManning", 0.0), ("bc_x", BC_PERIODIC),
+                ("bc_y", BC_PERIODIC), ("precision", FP64_FAST), ("device", 0),
+                ("bathy_kind", BATHY_NONE), ("bathy_par", ()), ("tables", None),
+                ("bathy_arrays", None))]
+            if kw:
+                raise TypeError(f"SGNBatch: unknown instance keys {sorted(kw)}")
+            holders.append(_DescHolder(*args))
+        n = len(holders)
+        descs = (_Desc * n)(*[h.desc for h in holders])
+        b = C.c_void_p()
+        rc = lib().sgnb_batch_create(descs, n, C.byref(b))
+        if rc != 0:
+            msg = lib().sgnb_batch_last_error(None)
+            raise SgnbError(rc, msg.decode() if msg else "")
+        self._b = b
+        self.n = n
+        self._views = []
+        for i, h in enumerate(holders):
+            d = h.desc
+            self._views.append(SGN2DB200(P=d.P, Nx=d.Nx, Ny=d.Ny, Lx=d.Lx, Ly=d.Ly,
+                                         precision=d.precision, device=device,
+                                         _handle=lib().sgnb_batch_instance(b, i)))
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().sgnb_batch_last_error(self._b)
+            raise SgnbError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if self._b:
+            for v in self._views:
+                v.close()
+            lib().sgnb_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return self.n
+
+    def __getitem__(self, i) -> SGN2DB200:
+        return self._views[i]
+
+    def integrate_steps(self, dt0, nsteps, opt: AdaptiveRKOptions | None = None):
+        """``nsteps`` accepted BS3(2) steps of every instance from step sizes ``dt0[i]``."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt0, dtype=np.float64), (self.n,)))
+        o = _Opts(**dataclasses.asdict(opt or AdaptiveRKOptions()))
+        st = (_Stats * self.n)()
+        self._check(lib().sgnb_batch_integrate_steps(self._b, _ptr(d), int(nsteps), C.byref(o),
+                                                     st))
+        return [_stats(s) for s in st]
+
+    @property
+    def config(self):
+        sh, bl = C.c_int(), C.c_int()
+        self._check(lib().sgnb_batch_get_config(self._b, C.byref(sh), C.byref(bl)))
+        return sh.value, bl.value
+
+    @config.setter
+    def config(self, value):
+        self._check(lib().sgnb_batch_set_config(self._b, int(value[0]), int(value[1])))
+
+    def autotune(self, dt0, reps=3):
+        """Times every (tile shape, grid) pair; keeps the fastest. Returns ms per attempt,
+        shape-major (3 shapes x grids of 1..4 CTAs per SM)."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt0, dtype=np.float64), (self.n,)))
+        ms = np.zeros(12)
+        self._check(lib().sgnb_batch_autotune(self._b, _ptr(d), int(reps), _ptr(ms)))
+        return ms.reshape(3, 4)

@@ -65,3 +65,56 @@ def cfg2_state_torch(Nx=2048, Ny=1024, Lx=40.0, Ly=20.0, seed=2, device="cuda"):
             eta += A * torch.sin(k * (x * math.cos(T) + y * math.sin(T)) + P)
         U[0, r0:r0 + ey.numel()] = H + eta
     return U.reshape(-1)
+
+
+# ---------------------------------------------------------------------------------------
+# Configuration 4: the batched sweep. 256 instances (numpy default_rng(4)), each on the
+# 20 x 10 basin with reflective walls: Nx ~ U{64..512} and Ny ~ U{32..256} drawn
+# independently, alpha ~ U[1.5, 6] (c = alpha sqrt(g H0)), still depth a 1.0 plane with an
+# elliptic shoal centred at (12, 5), semi-axes 4 x 3, crest depth ~ U[0.3, 0.9]
+# (BATHY_SHOAL profile). Incident wave: the Gaussian hump of configuration 1,
+# eta = 0.05 exp(-((x - 6)^2 + (y - 5)^2) / 0.5), placed up-slope of the shoal; zero velocity,
+# w = p = 0.
+# ---------------------------------------------------------------------------------------
+CFG4 = dict(n=256, Lx=20.0, Ly=10.0, H0=1.0, seed=4)
+
+
+def cfg4_instances(n=256, seed=4, nx_range=(64, 512), ny_range=(32, 256)):
+    """Solver keyword dicts of the sweep's instances (FP64_FAST, walls)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        Nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+        Ny = int(rng.integers(ny_range[0], ny_range[1] + 1))
+        alpha = float(rng.uniform(1.5, 6.0))
+        crest = float(rng.uniform(0.3, 0.9))
+        shoal = (CFG4["H0"], crest, 12.0, 5.0, 4.0, 3.0)
+        out.append(dict(P=4, Nx=Nx, Ny=Ny, Lx=CFG4["Lx"], Ly=CFG4["Ly"], g=G,
+                        c=alpha * math.sqrt(G * CFG4["H0"]), gamma=GAMMA, bc_x=1, bc_y=1,
+                        bathy_kind=3, bathy_par=shoal))
+    return out
+
+
+def hump_shoal_state_torch(kw, device="cuda"):
+    """Initial state of one sweep instance as a float64 torch tensor (var-major)."""
+    import torch
+
+    Nx, Ny, Lx, Ly = kw["Nx"], kw["Ny"], kw["Lx"], kw["Ly"]
+    shoal = kw["bathy_par"]
+    s = math.sqrt(3.0 / 7.0)
+    nodes = torch.tensor([-1.0, -s, 0.0, s, 1.0], dtype=torch.float64, device=device)
+    hx, hy = Lx / Nx, Ly / Ny
+    a = torch.arange(5, device=device).repeat(5)
+    b = torch.arange(5, device=device).repeat_interleave(5)
+    ex = torch.arange(Nx, device=device, dtype=torch.float64)
+    ey = torch.arange(Ny, device=device, dtype=torch.float64)
+    x = ex[None, :, None] * hx + 0.5 * hx * (nodes[a][None, None, :] + 1.0)
+    y = ey[:, None, None] * hy + 0.5 * hy * (nodes[b][None, None, :] + 1.0)
+    x, y = torch.broadcast_tensors(x, y)
+    dx, dy = (x - shoal[2]) / shoal[4], (y - shoal[3]) / shoal[5]
+    q = torch.clamp(1.0 - (dx * dx + dy * dy), min=0.0)
+    H = shoal[0] - (shoal[0] - shoal[1]) * q ** 3
+    eta = 0.05 * torch.exp(-((x - 6.0) ** 2 + (y - 5.0) ** 2) / 0.5)
+    U = torch.zeros(5, Ny, Nx, 25, dtype=torch.float64, device=device)
+    U[0] = H + eta
+    return U.reshape(-1)
