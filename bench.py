@@ -158,6 +158,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
 
     Nx, Ny, Lx, Ly = W.CFG2["Nx"], W.CFG2["Ny"], W.CFG2["Lx"], W.CFG2["Ly"]
+    if args.mesh:
+        Nx, Ny = args.mesh
     kw = W.cfg2_solver_args(Nx, Ny, Lx, Ly)
     prec = sgnb.FP64_FAST if args.precision == "fast" else sgnb.FP64_EXACT
     dof = 5 * 25 * Nx * Ny
@@ -257,7 +259,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "configuration 2: 2048x1024 P=4 (262,144,000 DOF), "
+            "config": {"workload": f"configuration 2: {Nx}x{Ny} P=4 ({dof:,} DOF), "
                                    "40x20 basin with reflective walls, elliptic shoal, "
                                    "8 random-phase sines; adaptive BS3(2) steps",
                        "mesh": [Nx, Ny], "dof": dof, "precision": f"fp64-{args.precision}",
@@ -379,6 +381,8 @@ def main():
     ap.add_argument("--impl", choices=["sgnb", "reference"], default="sgnb")
     ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mesh", type=int, nargs=2, metavar=("NX", "NY"), default=None,
+                    help="smaller mesh of the same workload, for profiler captures only")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

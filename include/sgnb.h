@@ -223,6 +223,30 @@ int sgnb_batch_get_config(const sgnb_batch* b, int* shape, int* blocks);
 int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_out);
 const char* sgnb_batch_last_error(const sgnb_batch* b);
 
+/* Adjoint (no reference counterpart). A frozen-dt BS3(2) trajectory of a context
+ * (SGNB_FP64_FAST or SGNB_FP64_EXACT) parameterised by the bathymetry as Nx * Ny element
+ * means (mapped to the depth statics by the bilinear cell interpolant, SGNB_BATHY_CELLS
+ * with Mx = Nx, My = Ny) and the initial free surface eta0 (Nd nodal values;
+ * h0 = H + eta0, zero velocity, w = p = 0). sgnb_adj_forward replaces the context's
+ * bathymetry, runs nsteps steps of sizes dts, records eta = h - H at the gauge nodes
+ * after every step (eta_out[n * ngauges + g], n = 0 .. nsteps-1 for the states after
+ * steps 1 .. nsteps) and keeps the state every checkpoint_every steps; the context then
+ * holds the final state. sgnb_adj_vjp takes the cotangent of those records and returns
+ * the gradients with respect to the element means and eta0 (checkpoint-and-recompute,
+ * hand-written VJP kernels of every right-hand-side phase and of the RK update). */
+typedef struct sgnb_adj sgnb_adj;
+int sgnb_adj_create(sgnb_ctx* ctx, long long nsteps, const double* dts, int ngauges,
+                    const long long* gauge_nodes, int checkpoint_every, sgnb_adj** out);
+int sgnb_adj_destroy(sgnb_adj* a);
+int sgnb_adj_forward(sgnb_adj* a, const double* means, const double* eta0, double* eta_out);
+int sgnb_adj_vjp(sgnb_adj* a, const double* eta_bar, double* grad_means, double* grad_eta0);
+/* VJP of the right-hand side at a host state U: Ubar = (dR/dU)^T Rbar and the cotangents
+ * of the context's depth statics (any of those pointers may be NULL; sizes as in
+ * sgnb_desc's arrays). */
+int sgnb_rhs_vjp(sgnb_ctx* ctx, const double* U, const double* Rbar, double* Ubar,
+                 double* Hnod_bar, double* Hx_bar, double* Hy_bar, double* HfaceX_bar,
+                 double* HfaceY_bar, double* HfaceXEnd_bar, double* HfaceYEnd_bar);
+
 const char* sgnb_status_string(int status);
 /* Message of the last failure on ctx (or of the last failed sgnb_create when NULL). */
 const char* sgnb_last_error(const sgnb_ctx* ctx);

@@ -74,6 +74,8 @@ def _load(path: str) -> C.CDLL:
     lib.or_ndof.argtypes = [C.c_void_p]
     lib.or_tables.argtypes = [C.c_void_p] + [_dp] * 7
     lib.or_bathymetry.argtypes = [C.c_void_p] + [_dp] * 7
+    if hasattr(lib, "or_set_bathymetry"):
+        lib.or_set_bathymetry.argtypes = [C.c_void_p] + [_dp] * 7
     lib.or_node_coords.argtypes = [C.c_void_p, _dp, _dp]
     lib.or_rhs.argtypes = [C.c_void_p, _dp, _dp]
     lib.or_rhs.restype = C.c_int
@@ -140,6 +142,14 @@ class Oracle:
         self.lib.or_bathymetry(self.h, *(_ptr(out[k]) for k in (
             "Hnod", "Hx", "Hy", "HfaceX", "HfaceY", "HfaceXEnd", "HfaceYEnd")))
         return out
+
+    def set_bathymetry(self, arrays):
+        """Replaces the depth statics (keys as returned by bathymetry(); missing keys keep
+        the current array). Restatement only."""
+        keys = ("Hnod", "Hx", "Hy", "HfaceX", "HfaceY", "HfaceXEnd", "HfaceYEnd")
+        keep = [np.ascontiguousarray(arrays[k], dtype=np.float64) if k in arrays else None
+                for k in keys]
+        self.lib.or_set_bathymetry(self.h, *(_ptr(a) if a is not None else None for a in keep))
 
     def node_coords(self):
         x, y = np.zeros(self.Nd), np.zeros(self.Nd)

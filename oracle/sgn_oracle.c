@@ -368,6 +368,19 @@ void or_bathymetry(const or_ctx* s, double* Hnod, double* Hx, double* Hy, double
   if (HfaceYEnd) memcpy(HfaceYEnd, s->HfaceYEnd, (size_t)s->Nx * s->np * sizeof(double));
 }
 
+void or_set_bathymetry(or_ctx* s, const double* Hnod, const double* Hx, const double* Hy,
+                       const double* HfaceX, const double* HfaceY, const double* HfaceXEnd,
+                       const double* HfaceYEnd) {
+  const size_t nf = (size_t)s->ne * s->np;
+  if (Hnod) memcpy(s->Hnod, Hnod, s->Nd * sizeof(double));
+  if (Hx) memcpy(s->Hx, Hx, s->Nd * sizeof(double));
+  if (Hy) memcpy(s->Hy, Hy, s->Nd * sizeof(double));
+  if (HfaceX) memcpy(s->HfaceX, HfaceX, nf * sizeof(double));
+  if (HfaceY) memcpy(s->HfaceY, HfaceY, nf * sizeof(double));
+  if (HfaceXEnd) memcpy(s->HfaceXEnd, HfaceXEnd, (size_t)s->Ny * s->np * sizeof(double));
+  if (HfaceYEnd) memcpy(s->HfaceYEnd, HfaceYEnd, (size_t)s->Nx * s->np * sizeof(double));
+}
+
 /* ------------------------------------------------------------------------- */
 /* rhs: src/solver/sgn2d.cpp:125-290                                          */
 /* ------------------------------------------------------------------------- */

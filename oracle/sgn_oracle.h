@@ -51,6 +51,12 @@ void or_tables(const or_ctx* s, double* nodes, double* D, double* lL, double* lR
  * domain edges, used only by walls; any pointer may be NULL. */
 void or_bathymetry(const or_ctx* s, double* Hnod, double* Hx, double* Hy, double* HfaceX,
                    double* HfaceY, double* HfaceXEnd, double* HfaceYEnd);
+/* [restatement only] Replaces the bathymetry arrays (same sizes as or_bathymetry; NULL
+ * keeps an array). The tests perturb the depth statics directly through it when they
+ * check the adjoint of the right-hand side by finite differences. */
+void or_set_bathymetry(or_ctx* s, const double* Hnod, const double* Hx, const double* Hy,
+                       const double* HfaceX, const double* HfaceY, const double* HfaceXEnd,
+                       const double* HfaceYEnd);
 void or_node_coords(const or_ctx* s, double* x, double* y); /* sgn2d.cpp:89-102 */
 
 int or_rhs(const or_ctx* s, const double* U, double* dU);     /* sgn2d.cpp:125-290 */

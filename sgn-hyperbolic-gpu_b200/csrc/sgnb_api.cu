@@ -7,9 +7,7 @@
 // (stage 2, stage 3, end-point stage, controller); the host reads the controller back
 // once per chunk instead of once per step (the reference copies error partials to the
 // host every step, src/cuda/sgn2d_cuda.cu:506-516).
-#include "sgnb.h"
-#include "sgnb_device.h"
-#include "sgnb_setup.h"
+#include "sgnb_ctx.h"
 
 #include <cmath>
 #include <cstdio>
@@ -19,40 +17,6 @@
 
 using namespace sgnb;
 
-struct sgnb_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  sgnb_desc desc{};
-  int precision = SGNB_FP64_EXACT;
-  Mesh mesh;
-  FrTables tab;
-  long long Nd = 0, ntot = 0;
-  RhsConsts C{};
-  double* Hbuf = nullptr;  // one allocation holding all statics
-  double* U[2] = {nullptr, nullptr};
-  // stage derivatives: FP64 (exact / fast) or FP32 (mixed precision)
-  void* K1[2] = {nullptr, nullptr};
-  void* K2 = nullptr;
-  void* K3 = nullptr;
-  bool mixed = false;
-  double* partials = nullptr;
-  int nblk = 0;
-  double* diag = nullptr;  // diagnostic partials
-  int ndiag = 0;
-  CtrlState* dctrl = nullptr;
-  CtrlState* hctrl = nullptr;  // pinned mirror
-  double* dtList = nullptr;
-  long long dtCap = 0;
-  double* alog = nullptr;  // device attempt log of the last integration
-  static constexpr long long kLogCap = 1 << 16;
-  cudaGraphExec_t chunk = nullptr;
-  int chunkLen = 0;
-  cudaEvent_t evRead = nullptr;
-  long long launches = 0;  // kernels launched by the last integration
-  long long pendingMaxAccepted = 0;  // set by sgnb_integrate_steps
-  int cur = 0;
-  std::string err;
-};
 
 namespace {
 

@@ -96,7 +96,58 @@ struct BatchArgs {
   double coef;
 };
 
+// Vector-Jacobian product of R at a stage input y = u (k == nullptr) or u + acoef k,
+// with the cotangent alpha ra + beta rb (rb optional). Scratch written by the line
+// kernels and read by the gather kernel:
+//   Ub[d]   [5 Nd]   cotangent of each node from its direction-d line
+//   Hb[d]   [Nd]     nodal-depth cotangent from the direction-d lines
+//   Hxb,Hyb [Nd]     cotangents of dH/dx, dH/dy (x lines: sources)
+//   Sn[d][f][5 ne 5] cotangent of the neighbour's trace node across face f (0 low,
+//                    1 high) of line (e, j), field-minor
+//   Hf[d][f][5 ne]   cotangent of the face depth of face f of line (e, j)
+struct VjpArgs {
+  const double* u;
+  const double* k;
+  double acoef;
+  const double* ra;
+  const double* rb;
+  double alpha, beta;
+  double* Ub[2];
+  double* Hb[2];
+  double* Hxb;
+  double* Hyb;
+  double* Sn[2][2];
+  double* Hf[2][2];
+};
+
+// Outputs of the gather: ybar (optional) = the node cotangent of R's input;
+// uacc = lam + ybar (init; lam optional) or uacc += ybar; statics accumulators +=.
+struct GatherArgs {
+  double* ybar;
+  double* uacc;
+  const double* lam;
+  int init;
+  double* Hacc;
+  double* Hxacc;
+  double* Hyacc;
+  double* HfXacc;
+  double* HfYacc;
+  double* HfXEndacc;
+  double* HfYEndacc;
+};
+
 namespace dev {
+// Adjoint kernels (FP64, fast arithmetic).
+cudaError_t launch_vjp_rhs(const RhsConsts& C, const FrTablesDev& T, const VjpArgs& A,
+                           const GatherArgs& G, cudaStream_t s);
+cudaError_t launch_rk_update(const double* u, const double* k1, const double* k2,
+                             const double* k3, const double* dts, long long step, double* out,
+                             long long n, cudaStream_t s);
+cudaError_t launch_gauges(const double* U, const double* Hnod, const long long* nodes, int ng,
+                          double* eta, cudaStream_t s);
+cudaError_t launch_gauges_back(double* lam, const long long* nodes, int ng, const double* etab,
+                               cudaStream_t s);
+
 // Launchers (one translation unit per arithmetic mode).
 cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
                                cudaStream_t s);

@@ -230,4 +230,70 @@ void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p,
     }
 }
 
+namespace {
+// The four cells and bilinear weights of the kind-5 interpolant at (x, y) (the same
+// index arithmetic as still_depth).
+void cell_weights(const double* p, double x, double y, int idx[4], double w[4]) {
+  const int Mx = (int)p[0], My = (int)p[1];
+  const double cx = p[2] / Mx, cy = p[3] / My;
+  const double sx = x / cx - 0.5, sy = y / cy - 0.5;
+  const double fx0 = std::floor(sx), fy0 = std::floor(sy);
+  const double tx = sx - fx0, ty = sy - fy0;
+  int i0 = (int)fx0, j0 = (int)fy0;
+  int i1 = i0 + 1, j1 = j0 + 1;
+  i0 = ((i0 % Mx) + Mx) % Mx; i1 = ((i1 % Mx) + Mx) % Mx;
+  j0 = ((j0 % My) + My) % My; j1 = ((j1 % My) + My) % My;
+  idx[0] = i0 + Mx * j0; w[0] = (1.0 - tx) * (1.0 - ty);
+  idx[1] = i1 + Mx * j0; w[1] = tx * (1.0 - ty);
+  idx[2] = i0 + Mx * j1; w[2] = (1.0 - tx) * ty;
+  idx[3] = i1 + Mx * j1; w[3] = tx * ty;
+}
+}  // namespace
+
+void cells_transpose(const Mesh& m, const FrTables& t, const double* p, const Bathymetry& bar,
+                     double* means_bar) {
+  const int np = t.P + 1, npp = np * np;
+  const long long ne = (long long)m.Nx * m.Ny, Nd = ne * npp;
+  const int Mx = (int)p[0], My = (int)p[1];
+  for (long long i = 0; i < (long long)Mx * My; ++i) means_bar[i] = 0.0;
+  // nodal gradients are D H / J along the element's lines: move their cotangents to H
+  std::vector<double> Hn(bar.Hnod.begin(), bar.Hnod.end());
+  const double Jx = 0.5 * m.hx, Jy = 0.5 * m.hy;
+  for (long long e = 0; e < ne; ++e) {
+    double* He = Hn.data() + e * npp;
+    const double* gx = bar.Hx.data() + e * npp;
+    const double* gy = bar.Hy.data() + e * npp;
+    for (int b = 0; b < np; ++b)
+      for (int a = 0; a < np; ++a)
+        for (int k = 0; k < np; ++k) {
+          He[k + np * b] += t.D[a * np + k] * gx[a + np * b] / Jx;
+          He[a + np * k] += t.D[b * np + k] * gy[a + np * b] / Jy;
+        }
+  }
+  auto add = [&](double x, double y, double g) {
+    int idx[4];
+    double w[4];
+    cell_weights(p, x, y, idx, w);
+    for (int q = 0; q < 4; ++q) means_bar[idx[q]] += w[q] * g;
+  };
+  std::vector<double> x(Nd), y(Nd);
+  node_coords(m, t, x.data(), y.data());
+  for (long long i = 0; i < Nd; ++i) add(x[i], y[i], Hn[i]);
+  for (long long e = 0; e < ne; ++e) {
+    const int ex = (int)(e % m.Nx), ey = (int)(e / m.Nx);
+    for (int s = 0; s < np; ++s) {
+      const double yt = ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0);
+      const double xt = ex * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
+      add(ex * m.hx, yt, bar.HfX[e * np + s]);
+      add(xt, ey * m.hy, bar.HfY[e * np + s]);
+    }
+  }
+  for (int ey = 0; ey < m.Ny; ++ey)
+    for (int s = 0; s < np; ++s)
+      add(m.Nx * m.hx, ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0), bar.HfXEnd[(size_t)ey * np + s]);
+  for (int ex = 0; ex < m.Nx; ++ex)
+    for (int s = 0; s < np; ++s)
+      add(ex * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0), m.Ny * m.hy, bar.HfYEnd[(size_t)ex * np + s]);
+}
+
 }  // namespace sgnb

@@ -29,5 +29,9 @@ double still_depth(int kind, const double* p, double x, double y);
 int bathy_param_count(int kind, const double* p, int n);
 void node_coords(const Mesh& m, const FrTables& t, double* x, double* y);
 void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p, Bathymetry& out);
+// Transpose of bathymetry() for kind 5 (cell means p = {Mx, My, Lx, Ly, means...}):
+// cotangents of every static (bar) -> cotangent of the Mx * My means.
+void cells_transpose(const Mesh& m, const FrTables& t, const double* p, const Bathymetry& bar,
+                     double* means_bar);
 
 }  // namespace sgnb

@@ -150,6 +150,12 @@ SIGNATURES = {
     "sgnb_batch_get_config": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "sgnb_batch_autotune": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp]),
     "sgnb_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "sgnb_adj_create": (C.c_int, [C.c_void_p, C.c_longlong, _dp, C.c_int,
+                                  C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_void_p)]),
+    "sgnb_adj_destroy": (C.c_int, [C.c_void_p]),
+    "sgnb_adj_forward": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "sgnb_adj_vjp": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "sgnb_rhs_vjp": (C.c_int, [C.c_void_p, _dp, _dp, _dp] + [_dp] * 7),
     "sgnb_status_string": (C.c_char_p, [C.c_int]),
     "sgnb_last_error": (C.c_char_p, [C.c_void_p]),
 }
@@ -418,6 +424,20 @@ class SGN2DB200:
         n = C.c_longlong()
         _check(lib().sgnb_attempt_log(self._h, _ptr(buf), cap, C.byref(n)), self._h)
         return buf[: 4 * min(n.value, cap)].reshape(-1, 4)
+
+    def rhs_vjp(self, U, Rbar):
+        """(dR/dU)^T Rbar at the host state U and the cotangents of the depth statics
+        (dict with the keys of setup_bathymetry)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        Rbar = np.ascontiguousarray(Rbar, dtype=np.float64)
+        Ub = np.empty(self.n)
+        Nd, nf = self.Nd, 5 * self.Nx * self.Ny
+        bars = dict(Hnod=np.zeros(Nd), Hx=np.zeros(Nd), Hy=np.zeros(Nd), HfaceX=np.zeros(nf),
+                    HfaceY=np.zeros(nf), HfaceXEnd=np.zeros(5 * self.Ny),
+                    HfaceYEnd=np.zeros(5 * self.Nx))
+        _check(lib().sgnb_rhs_vjp(self._h, _ptr(U), _ptr(Rbar), _ptr(Ub), *(_ptr(bars[k]) for k in (
+            "Hnod", "Hx", "Hy", "HfaceX", "HfaceY", "HfaceXEnd", "HfaceYEnd"))), self._h)
+        return Ub, bars
 
     # --- diagnostics -------------------------------------------------------------
     def _scalar(self, fn, *args):

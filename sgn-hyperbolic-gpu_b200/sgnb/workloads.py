@@ -118,3 +118,60 @@ def hump_shoal_state_torch(kw, device="cuda"):
     U = torch.zeros(5, Ny, Nx, 25, dtype=torch.float64, device=device)
     U[0] = H + eta
     return U.reshape(-1)
+
+
+# ---------------------------------------------------------------------------------------
+# Configuration 5: the adjoint. 256 x 128 elements on the 20 x 10 basin with reflective
+# walls, alpha = 3 (c = 3 sqrt(g)), FP64. Bathymetry: 32,768 element means, the elliptic
+# shoal of configuration 4 (plane 1.0, crest 0.5 at (12, 5), semi-axes 4 x 3) sampled at
+# the element centres plus seeded noise of standard deviation 0.005 (numpy
+# default_rng(5)); mapped to the nodes by the bilinear cell interpolant (BATHY_CELLS).
+# Initial free surface: the Gaussian hump 0.05 exp(-((x - 6)^2 + (y - 5)^2) / 0.5).
+# 16 gauges at the nearest nodes of seeded uniform positions. Target: the run from means
+# perturbed by seeded noise of standard deviation 0.01 and a hump 10 % higher. The 200
+# step sizes come from an adaptive run of the unperturbed problem (atol 1e-8, rtol 1e-6)
+# and are then frozen; checkpoints every 20 steps.
+# ---------------------------------------------------------------------------------------
+CFG5 = dict(Nx=256, Ny=128, Lx=20.0, Ly=10.0, steps=200, gauges=16, checkpoint=20, seed=5)
+
+
+def gll_nodes():
+    s = math.sqrt(3.0 / 7.0)
+    return np.array([-1.0, -s, 0.0, s, 1.0])
+
+
+def node_coords_np(Nx, Ny, Lx, Ly):
+    """Node coordinates in the solver's layout (e * 25 + a + 5 b), numpy."""
+    xi = gll_nodes()
+    hx, hy = Lx / Nx, Ly / Ny
+    a = np.tile(np.arange(5), 5)
+    b = np.repeat(np.arange(5), 5)
+    ex = np.arange(Nx)
+    ey = np.arange(Ny)
+    x = ex[None, :, None] * hx + 0.5 * hx * (xi[a][None, None, :] + 1.0)
+    y = ey[:, None, None] * hy + 0.5 * hy * (xi[b][None, None, :] + 1.0)
+    x, y = np.broadcast_arrays(x, y)
+    return x.reshape(-1).copy(), y.reshape(-1).copy()
+
+
+def cfg5_problem(Nx=256, Ny=128, Lx=20.0, Ly=10.0, ngauges=16, seed=5):
+    """Means, eta0, gauge nodes, the target's parameters and the solver arguments."""
+    rng = np.random.default_rng(seed)
+    cx = (np.arange(Nx) + 0.5) * Lx / Nx
+    cy = (np.arange(Ny) + 0.5) * Ly / Ny
+    X, Y = np.meshgrid(cx, cy)
+    r2 = ((X - 12.0) / 4.0) ** 2 + ((Y - 5.0) / 3.0) ** 2
+    q = np.clip(1.0 - r2, 0.0, None)
+    means = (1.0 - 0.5 * q ** 3 + 0.005 * rng.standard_normal(X.shape)).reshape(-1)
+    x, y = node_coords_np(Nx, Ny, Lx, Ly)
+    eta0 = 0.05 * np.exp(-((x - 6.0) ** 2 + (y - 5.0) ** 2) / 0.5)
+    gx = rng.uniform(0.0, Lx, ngauges)
+    gy = rng.uniform(0.0, Ly, ngauges)
+    gauges = np.array([int(np.argmin((x - px) ** 2 + (y - py) ** 2)) for px, py in zip(gx, gy)],
+                      dtype=np.int64)
+    target_means = means + 0.01 * rng.standard_normal(means.shape)
+    target_eta0 = 1.1 * eta0
+    kw = dict(P=4, Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, g=G, c=ALPHA * math.sqrt(G * 1.0), gamma=GAMMA,
+              bc_x=1, bc_y=1, bathy_kind=5, bathy_par=np.concatenate([[Nx, Ny, Lx, Ly], means]))
+    return dict(kw=kw, means=means, eta0=eta0, gauges=gauges, target_means=target_means,
+                target_eta0=target_eta0)
