@@ -46,6 +46,14 @@ BYTES_PER_DOF = {
 }
 
 
+# Mixed precision: FP64 state, FP32 stage derivatives (4 B), FP64 statics.
+BYTES_PER_DOF_MIXED = {
+    "rhs": 16.0 + STATIC_B,                  # FP64 in and out (rhs callers): 21.44
+    "stage": 8 + 4 + STATIC_B + 4,           # u (8), k (4) in; k_out (4): 21.44
+    "fsal": 8 + 3 * 4 + STATIC_B + 8 + 4,    # u, k1..k3 in; uNew (8), k4 (4) out: 37.44
+}
+
+
 def measured_peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -161,7 +169,7 @@ def run_ours(args):
     if args.mesh:
         Nx, Ny = args.mesh
     kw = W.cfg2_solver_args(Nx, Ny, Lx, Ly)
-    prec = sgnb.FP64_FAST if args.precision == "fast" else sgnb.FP64_EXACT
+    prec = {"fast": sgnb.FP64_FAST, "exact": sgnb.FP64_EXACT, "mixed": sgnb.MIXED}[args.precision]
     dof = 5 * 25 * Nx * Ny
     Ud = W.cfg2_state_torch(Nx, Ny, Lx, Ly, device=f"cuda:{local}")
     U_host = torch.empty(Ud.numel(), dtype=torch.float64, pin_memory=True)
@@ -215,14 +223,15 @@ def run_ours(args):
         per[key] = a0.elapsed_time(a1) / 1e3 / reps
     dominant = "fsal" if per["fsal"] >= 2 * per["stage"] else "stage"
     peak, peak_kind = measured_peak_hbm()
-    achieved = BYTES_PER_DOF[dominant] * dof / per[dominant] / 1e9
+    bpd = BYTES_PER_DOF_MIXED if args.precision == "mixed" else BYTES_PER_DOF
+    achieved = bpd[dominant] * dof / per[dominant] / 1e9
     tpd = traffic_per_dof()
-    traffic = tpd.get(dominant)
+    traffic = tpd.get(dominant) if args.precision != "mixed" else None
     roofline = {"bound": "hbm", "kernel": f"k_fused ({dominant} mode)",
                 "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": (round(traffic * dof) if traffic else None),
-                "algorithmic_bytes": round(BYTES_PER_DOF[dominant] * dof),
+                "algorithmic_bytes": round(bpd[dominant] * dof),
                 "launch_ms": {k: round(v * 1e3, 4) for k, v in per.items()}}
 
     # ---- e2e through the public API with host buffers ----------------------------
@@ -258,7 +267,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 state, f32 deviations" if args.precision == "mixed" else "f64",
+            "data": "synthetic",
             "config": {"workload": f"configuration 2: {Nx}x{Ny} P=4 ({dof:,} DOF), "
                                    "40x20 basin with reflective walls, elliptic shoal, "
                                    "8 random-phase sines; adaptive BS3(2) steps",
@@ -379,7 +390,13 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["sgnb", "reference"], default="sgnb")
-    ap.add_argument("--precision", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--precision", choices=["fast", "exact", "mixed"], default="fast")
+    ap.add_argument("--workload", choices=["cfg2", "sweep", "mixed", "adjoint"],
+                    default="cfg2",
+                    help="cfg2: the benchmark (default); sweep: the 256-instance batched "
+                         "sweep against sequential single-instance runs; mixed: mixed vs "
+                         "FP64 on configuration 2 with the eta error; adjoint: "
+                         "configuration 5 forward + VJP")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mesh", type=int, nargs=2, metavar=("NX", "NY"), default=None,
                     help="smaller mesh of the same workload, for profiler captures only")
@@ -388,6 +405,15 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "sweep":
+        from sgnb import benchmarks as BW
+        BW.run_sweep(args, ClockSampler, measured_peak_hbm())
+    elif args.workload == "mixed":
+        from sgnb import benchmarks as BW
+        BW.run_mixed(args, ClockSampler, measured_peak_hbm())
+    elif args.workload == "adjoint":
+        from sgnb import benchmarks as BW
+        BW.run_adjoint(args, ClockSampler, measured_peak_hbm())
     else:
         run_ours(args)
 

@@ -208,18 +208,23 @@ typedef struct sgnb_batch sgnb_batch;
 int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out);
 int sgnb_batch_destroy(sgnb_batch* b);
 int sgnb_batch_size(const sgnb_batch* b);
+/* The batch's CUDA stream (cudaStream_t): its launches run there, for callers that time or
+ * order work around them. */
+int sgnb_batch_stream(const sgnb_batch* b, void** stream);
 sgnb_ctx* sgnb_batch_instance(sgnb_batch* b, int i);
 /* nsteps accepted steps for every instance, starting from dt0[i]; stats[n]. */
 int sgnb_batch_integrate_steps(sgnb_batch* b, const double* dt0, long long nsteps,
                                const sgnb_rk_opts* opts, sgnb_rk_stats* stats);
-/* Launch configuration: tile shape (0: 8x4, 1: 16x2, 2: 4x8 elements) and the number of
- * persistent CTAs (default: 8x4, two CTAs per SM; sgnb_batch_autotune picks one). */
+/* Launch configuration: tile shape (0: 8x4, 1: 16x2, 2: 4x8 elements) and the grid:
+ * blocks == 0 launches one CTA per tile of the work list, blocks > 0 that many persistent
+ * CTAs looping over it (default: 8x4, one CTA per tile; sgnb_batch_autotune picks one). */
 int sgnb_batch_set_config(sgnb_batch* b, int shape, int blocks);
 int sgnb_batch_get_config(const sgnb_batch* b, int* shape, int* blocks);
 /* Autotuner: times one adaptive attempt (three stage launches, reps times) for every tile
- * shape and persistent grids of 1..4 CTAs per SM at step sizes dt0[i], keeps the fastest
- * (sgnb_batch_get_config reports it). ms_out (optional, 12 entries, shape-major) receives
- * the measured ms per attempt. The instances' states are left unchanged. */
+ * shape and grid (one CTA per tile, persistent grids of 1..4 CTAs per SM) at step sizes
+ * dt0[i], keeps the fastest (sgnb_batch_get_config reports it). ms_out (optional, 15
+ * entries, shape-major) receives the measured ms per attempt. The instances' states are
+ * left unchanged. */
 int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_out);
 const char* sgnb_batch_last_error(const sgnb_batch* b);
 

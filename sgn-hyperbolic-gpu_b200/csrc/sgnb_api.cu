@@ -638,7 +638,9 @@ const char* sgnb_last_error(const sgnb_ctx* c) {
 // ===========================================================================
 // Batched sweep: many independent instances, one persistent launch per RK stage.
 // ===========================================================================
-constexpr int kTuneFactors = 4;  // persistent grids of 1..4 CTAs per SM
+// launch configurations the autotuner tries per tile shape: one CTA per tile (grid
+// option 0), then persistent grids of 1..4 CTAs per SM (options 1..4)
+constexpr int kTuneGrids = 5;
 
 struct sgnb_batch {
   int n = 0;
@@ -856,7 +858,7 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   b->shape = 0;
-  b->blocks = 2 * sms;
+  b->blocks = 0;
   *out = b;
   return SGNB_OK;
 }
@@ -882,12 +884,18 @@ int sgnb_batch_destroy(sgnb_batch* b) {
 
 int sgnb_batch_size(const sgnb_batch* b) { return b ? b->n : 0; }
 
+int sgnb_batch_stream(const sgnb_batch* b, void** stream) {
+  if (!b || !stream) return SGNB_ERR_INVALID;
+  *stream = (void*)b->stream;
+  return SGNB_OK;
+}
+
 sgnb_ctx* sgnb_batch_instance(sgnb_batch* b, int i) {
   return (b && i >= 0 && i < b->n) ? b->ctx[i] : nullptr;
 }
 
 int sgnb_batch_set_config(sgnb_batch* b, int shape, int blocks) {
-  if (!b || shape < 0 || shape > 2 || blocks < 1) return bfail(b, SGNB_ERR_INVALID, "shape 0..2, blocks >= 1");
+  if (!b || shape < 0 || shape > 2 || blocks < 0) return bfail(b, SGNB_ERR_INVALID, "shape 0..2, blocks >= 0");
   b->shape = shape;
   b->blocks = blocks;
   return SGNB_OK;
@@ -966,10 +974,10 @@ int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_o
   SGNB_BCU(b, cudaEventCreate(&e0));
   SGNB_BCU(b, cudaEventCreate(&e1));
   double best = 1e300;
-  int bestShape = 0, bestBlocks = 2 * sms;
+  int bestShape = 0, bestBlocks = 0;
   int rc = SGNB_OK;
   for (int sh = 0; sh < 3 && rc == SGNB_OK; ++sh) {
-    for (int f = 1; f <= kTuneFactors && rc == SGNB_OK; ++f) {
+    for (int f = 0; f < kTuneGrids && rc == SGNB_OK; ++f) {
       const int blocks = f * sms;
       auto run = [&](int count) {
         cudaError_t e = cudaSuccess;
@@ -991,7 +999,7 @@ int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_o
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
       if (e != cudaSuccess) { rc = bfail(b, SGNB_ERR_CUDA, std::string("autotune: ") + cudaGetErrorName(e)); break; }
       const double per = (double)ms / reps;
-      if (ms_out) ms_out[sh * kTuneFactors + (f - 1)] = per;
+      if (ms_out) ms_out[sh * kTuneGrids + f] = per;
       if (per < best) { best = per; bestShape = sh; bestBlocks = blocks; }
     }
   }

@@ -159,8 +159,8 @@ cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A
                                cudaStream_t s);
 cudaError_t prepare_fused_mixed();
 int fused_grid_blocks(int Nx, int Ny);
-// Batched launch (FP64 fast): tile shape shape_id (0: 8x4, 1: 16x2, 2: 4x8), grid of
-// `blocks` persistent CTAs.
+// Batched launch (FP64 fast): tile shape shape_id (0: 8x4, 1: 16x2, 2: 4x8); `blocks`
+// persistent CTAs looping over the work list, or one CTA per tile when blocks == 0.
 cudaError_t launch_fused_batch(int mode, int shape_id, int blocks, const BatchArgs& B,
                                cudaStream_t s);
 cudaError_t prepare_fused_batch();

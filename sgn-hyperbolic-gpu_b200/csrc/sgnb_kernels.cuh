@@ -180,13 +180,14 @@ struct Prim {
 // Hydrostatic part 0.5 g (h^2 - H^2) of the normal momentum flux. h^2 - H^2 cancels
 // where h ~ H; both modes round the two squares separately, as the CPU does, because
 // the derivative amplifies this term's rounding by ~|D|/J.
-__device__ __forceinline__ double hydro(const RhsConsts& C, double h, double Hloc) {
+template <class TC>
+__device__ __forceinline__ double hydro(const TC& C, double h, double Hloc) {
   return C.halfg * (__dmul_rn(h, h) - __dmul_rn(Hloc, Hloc));
 }
 
 // Normal-momentum component of the directional flux (sgn_flux2d.h:94, 109).
-template <bool EXACT, int DIR>
-__device__ __forceinline__ double flux_normal(const RhsConsts& C, const double* U,
+template <bool EXACT, int DIR, class TC>
+__device__ __forceinline__ double flux_normal(const TC& C, const double* U,
                                               const Prim<EXACT>& q, double Hloc) {
   const double hn = DIR == 0 ? U[1] : U[2];
   const double hp = EXACT ? U[0] * q.p : U[4];
@@ -194,8 +195,8 @@ __device__ __forceinline__ double flux_normal(const RhsConsts& C, const double* 
 }
 
 // Directional flux: fluxX (DIR 0) or fluxY (DIR 1), src/physics/sgn_flux2d.h:89-116.
-template <bool EXACT, int DIR>
-__device__ __forceinline__ void flux(const RhsConsts& C, const double* U, const Prim<EXACT>& q,
+template <bool EXACT, int DIR, class TC>
+__device__ __forceinline__ void flux(const TC& C, const double* U, const Prim<EXACT>& q,
                                      double Hloc, double* F) {
   const double hn = DIR == 0 ? U[1] : U[2];  // normal discharge
   F[0] = hn;
@@ -211,8 +212,8 @@ __device__ __forceinline__ void flux(const RhsConsts& C, const double* U, const 
 }
 
 // |normal velocity| + sqrt(max(g h + p + c^2, 0)), src/physics/sgn_flux2d.h:73-86.
-template <bool EXACT, int DIR>
-__device__ __forceinline__ double wave_speed(const RhsConsts& C, const double* U,
+template <bool EXACT, int DIR, class TC>
+__device__ __forceinline__ double wave_speed(const TC& C, const double* U,
                                              const Prim<EXACT>& q) {
   const double arg = C.g * U[0] + q.p + C.c2;
   const double ce = sqrt(arg > 0.0 ? arg : 0.0);
@@ -221,8 +222,8 @@ __device__ __forceinline__ double wave_speed(const RhsConsts& C, const double* U
 
 // Field v of the directional flux from the per-node quantities: normal discharge hn,
 // primitives q and the precomputed normal-momentum component fn (sgn_flux2d.h:89-116).
-template <bool EXACT, int DIR>
-__device__ __forceinline__ double flux_field(const RhsConsts& C, int v, double hn,
+template <bool EXACT, int DIR, class TC>
+__device__ __forceinline__ double flux_field(const TC& C, int v, double hn,
                                              const Prim<EXACT>& q, double fn) {
   switch (v) {
     case 0: return hn;
@@ -246,8 +247,8 @@ __device__ __forceinline__ double flux_field(const RhsConsts& C, int v, double h
 // derivative of node m, then emit(m, v, d, q) with the FR-corrected derivative of flux
 // field v at node m (both already divided by J). The flux of each field is rebuilt from
 // per-node quantities inside the contraction, which keeps the live set small.
-template <bool EXACT, int DIR, class TB, class EmitH, class Emit>
-__device__ __forceinline__ void line_pass(const RhsConsts& C, const TB& Tb, const double (&Un)[NP][NV],
+template <bool EXACT, int DIR, class TC, class TB, class EmitH, class Emit>
+__device__ __forceinline__ void line_pass(const TC& C, const TB& Tb, const double (&Un)[NP][NV],
                                           const double (&Hn)[NP], const double* nLo,
                                           const double* nHi, double HfLo, double HfHi,
                                           EmitH&& emit_dh, Emit&& emit) {
@@ -363,8 +364,8 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 // One tile of the fused right-hand side / stage kernel: tile (bx, by) of the mesh whose
 // constants are C, error partial slot blk. Shared by the single-instance kernel and the
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
-template <int MODE, bool EXACT, int TX_, int TY_, class TB>
-__device__ __forceinline__ void fused_tile(const RhsConsts& C, const TB& Tb, const StageArgs& A,
+template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA>
+__device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_>::Smem& S) {
   using T = Tile<TX_, TY_>;
@@ -392,7 +393,11 @@ __device__ __forceinline__ void fused_tile(const RhsConsts& C, const TB& Tb, con
   I.k2 = A.K2;
   I.k3 = A.K3;
 
-  const int tid = threadIdx.x;
+  // the thread index read through an opaque move: in the persistent batched kernel this
+  // keeps the compiler from hoisting the per-thread item and halo descriptors out of the
+  // tile loop (they would stay live, in registers, across every tile's passes)
+  int tid;
+  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
   const int warp = tid >> 5, lane = tid & 31;
   const int Nx = C.Nx, Ny = C.Ny;
   const long long Nd = C.Nd;
@@ -795,11 +800,43 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const Stag
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
-// Batched form: one persistent launch walks the tiles of many independent instances
+// Batched form: one launch per stage walks the tiles of many independent instances
 // (the work list tile_inst / tile_start), each with its own constants, buffers and
 // controller. The instance's constants and buffer pointers are copied into shared
-// memory once per tile.
+// memory once per tile. PERSIST: a fixed grid of CTAs loops over the work list;
+// otherwise one CTA per tile (no loop: the compiler then keeps nothing live from one tile
+// to the next, which the loop costs in spilled registers).
 template <int MODE, bool EXACT, int TX_, int TY_>
+__device__ __forceinline__ void batch_tile(const BatchArgs& B, long long t,
+                                           typename Tile<TX_, TY_>::Smem& S, RhsConsts& Cs,
+                                           StageArgs& As) {
+  const int inst = B.tile_inst[t];
+  const long long lt = t - B.tile_start[inst];
+  __syncthreads();  // the previous tile is done with Cs / As
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(B.consts + inst);
+    unsigned* dst = reinterpret_cast<unsigned*>(&Cs);
+    for (int w = threadIdx.x; w < (int)(sizeof(RhsConsts) / 4); w += NTHR) dst[w] = src[w];
+    const unsigned* srca = reinterpret_cast<const unsigned*>(B.args + inst);
+    unsigned* dsta = reinterpret_cast<unsigned*>(&As);
+    for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 4); w += NTHR) dsta[w] = srca[w];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    As.kin_k2 = B.kin_k2;
+    As.coef = B.coef;
+    if (MODE == MODE_STAGE) As.out = B.kin_k2 ? As.K3 : As.K2;
+  }
+  __syncthreads();
+  const int ntx = (Cs.Nx + TX_ - 1) / TX_;
+  // volatile views: per-instance values are re-read from shared memory at each use
+  // rather than held in registers through the passes
+  fused_tile<MODE, EXACT, TX_, TY_>(static_cast<const volatile RhsConsts&>(Cs), B.tables,
+                                    static_cast<const volatile StageArgs&>(As),
+                                    (int)(lt % ntx), (int)(lt / ntx), lt, S);
+}
+
+template <int MODE, bool EXACT, int TX_, int TY_, bool PERSIST>
 __global__ void __launch_bounds__(NTHR, 2) k_fused_batch(const BatchArgs B) {
   // FR tables come from the kernel parameters (constant bank): the same for every
   // instance (P = 4 GLL)
@@ -808,27 +845,11 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused_batch(const BatchArgs B) {
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
   __shared__ RhsConsts Cs;
   __shared__ StageArgs As;
-  for (long long t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
-    const int inst = B.tile_inst[t];
-    const long long lt = t - B.tile_start[inst];
-    __syncthreads();  // the previous tile is done with Cs / As
-    {
-      const unsigned* src = reinterpret_cast<const unsigned*>(B.consts + inst);
-      unsigned* dst = reinterpret_cast<unsigned*>(&Cs);
-      for (int w = threadIdx.x; w < (int)(sizeof(RhsConsts) / 4); w += NTHR) dst[w] = src[w];
-      const unsigned* srca = reinterpret_cast<const unsigned*>(B.args + inst);
-      unsigned* dsta = reinterpret_cast<unsigned*>(&As);
-      for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 4); w += NTHR) dsta[w] = srca[w];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      As.kin_k2 = B.kin_k2;
-      As.coef = B.coef;
-      if (MODE == MODE_STAGE) As.out = B.kin_k2 ? As.K3 : As.K2;
-    }
-    __syncthreads();
-    const int ntx = (Cs.Nx + TX_ - 1) / TX_;
-    fused_tile<MODE, EXACT, TX_, TY_>(Cs, B.tables, As, (int)(lt % ntx), (int)(lt / ntx), lt, S);
+  if constexpr (PERSIST) {
+    for (long long t = blockIdx.x; t < B.ntiles; t += gridDim.x)
+      batch_tile<MODE, EXACT, TX_, TY_>(B, t, S, Cs, As);
+  } else {
+    if ((long long)blockIdx.x < B.ntiles) batch_tile<MODE, EXACT, TX_, TY_>(B, blockIdx.x, S, Cs, As);
   }
 }
 

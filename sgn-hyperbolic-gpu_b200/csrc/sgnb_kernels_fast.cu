@@ -13,7 +13,13 @@ cudaError_t prepare_fused_fast() { return prepare_all(); }
 
 template <int MODE, int TXs, int TYs>
 static cudaError_t launch_b(int blocks, const BatchArgs& B, cudaStream_t s) {
-  k_fused_batch<MODE, false, TXs, TYs><<<blocks, NTHR, sizeof(typename Tile<TXs, TYs>::Smem), s>>>(B);
+  const size_t smem = sizeof(typename Tile<TXs, TYs>::Smem);
+  if (blocks > 0) {
+    k_fused_batch<MODE, false, TXs, TYs, true><<<blocks, NTHR, smem, s>>>(B);
+  } else {
+    if (B.ntiles < 1 || B.ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    k_fused_batch<MODE, false, TXs, TYs, false><<<(unsigned)B.ntiles, NTHR, smem, s>>>(B);
+  }
   return cudaGetLastError();
 }
 
@@ -39,18 +45,22 @@ cudaError_t launch_fused_batch(int mode, int shape_id, int blocks, const BatchAr
 
 int batch_tile_tx(int shape_id) { return shape_id == 1 ? 16 : (shape_id == 2 ? 4 : 8); }
 
+template <int MODE, int TXs, int TYs>
+static cudaError_t prepare_mode() {
+  const int bytes = (int)sizeof(typename Tile<TXs, TYs>::Smem);
+  cudaError_t e = cudaFuncSetAttribute(k_fused_batch<MODE, false, TXs, TYs, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_fused_batch<MODE, false, TXs, TYs, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 template <int TXs, int TYs>
 static cudaError_t prepare_shape() {
-  const int bytes = (int)sizeof(typename Tile<TXs, TYs>::Smem);
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_fused_batch<MODE_RHS, false, TXs, TYs>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
-    return e;
-  if ((e = cudaFuncSetAttribute(k_fused_batch<MODE_STAGE, false, TXs, TYs>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
-    return e;
-  return cudaFuncSetAttribute(k_fused_batch<MODE_FSAL, false, TXs, TYs>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = prepare_mode<MODE_RHS, TXs, TYs>();
+  if (e == cudaSuccess) e = prepare_mode<MODE_STAGE, TXs, TYs>();
+  if (e == cudaSuccess) e = prepare_mode<MODE_FSAL, TXs, TYs>();
+  return e;
 }
 
 cudaError_t prepare_fused_batch() {

@@ -144,6 +144,7 @@ SIGNATURES = {
     "sgnb_batch_destroy": (C.c_int, [C.c_void_p]),
     "sgnb_batch_size": (C.c_int, [C.c_void_p]),
     "sgnb_batch_instance": (C.c_void_p, [C.c_void_p, C.c_int]),
+    "sgnb_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sgnb_batch_integrate_steps": (C.c_int, [C.c_void_p, _dp, C.c_longlong, C.POINTER(_Opts),
                                              C.POINTER(_Stats)]),
     "sgnb_batch_set_config": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
@@ -544,6 +545,13 @@ class SGNBatch:
         return [_stats(s) for s in st]
 
     @property
+    def stream(self) -> int:
+        """The batch's CUDA stream handle (its launches run there)."""
+        sp = C.c_void_p()
+        self._check(lib().sgnb_batch_stream(self._b, C.byref(sp)))
+        return sp.value or 0
+
+    @property
     def config(self):
         sh, bl = C.c_int(), C.c_int()
         self._check(lib().sgnb_batch_get_config(self._b, C.byref(sh), C.byref(bl)))
@@ -555,8 +563,9 @@ class SGNBatch:
 
     def autotune(self, dt0, reps=3):
         """Times every (tile shape, grid) pair; keeps the fastest. Returns ms per attempt,
-        shape-major (3 shapes x grids of 1..4 CTAs per SM)."""
+        [3 shapes (8x4, 16x2, 4x8), 5 grids (one CTA per tile, 1..4 persistent CTAs per
+        SM)]."""
         d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt0, dtype=np.float64), (self.n,)))
-        ms = np.zeros(12)
+        ms = np.zeros(15)
         self._check(lib().sgnb_batch_autotune(self._b, _ptr(d), int(reps), _ptr(ms)))
-        return ms.reshape(3, 4)
+        return ms.reshape(3, 5)

