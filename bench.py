@@ -36,21 +36,21 @@ sys.path.insert(0, os.path.join(ROOT, "sgn-hyperbolic-gpu_b200"))
 
 METRIC = "DOF-updates/s per RK stage"
 UNIT = "DOF-updates/s"
-# Algorithmic HBM bytes per DOF (8 B doubles): U in and dU out (16), nodal H, Hx, Hy
-# (3 x 8 / 5 fields = 4.8), face depths (2 x 5 per element / 125 DOF x 8 = 0.64).
-STATIC_B = 4.8 + 0.64
+# Algorithmic HBM bytes per DOF (8 B doubles) of the fused kernels: U in and dU out (16),
+# the nodal depth H (8 / 5 fields = 1.6) and the face depths (2 x 5 per element / 125 DOF
+# x 8 = 0.64). The nodal depth gradients dH/dx, dH/dy (3.2 B/DOF more if read) are formed
+# from the depth tile in shared memory, so they are not part of the kernels' traffic.
+STATIC_B = 1.6 + 0.64
 BYTES_PER_DOF = {
-    "rhs": 16.0 + STATIC_B,                  # 21.44
-    "stage": 8 + 8 + STATIC_B + 8,           # u, k in; k_out out: 29.44
-    "fsal": 4 * 8 + STATIC_B + 2 * 8,        # u, k1..k3 in; uNew, k4 out: 53.44
+    "rhs": 16.0 + STATIC_B,                  # 18.24
+    "stage": 8 + 8 + STATIC_B + 8,           # u, k in; k_out out: 26.24
+    "fsal": 4 * 8 + STATIC_B + 2 * 8,        # u, k1..k3 in; uNew, k4 out: 50.24
 }
-
-
 # Mixed precision: FP64 state, FP32 stage derivatives (4 B), FP64 statics.
 BYTES_PER_DOF_MIXED = {
-    "rhs": 16.0 + STATIC_B,                  # FP64 in and out (rhs callers): 21.44
-    "stage": 8 + 4 + STATIC_B + 4,           # u (8), k (4) in; k_out (4): 21.44
-    "fsal": 8 + 3 * 4 + STATIC_B + 8 + 4,    # u, k1..k3 in; uNew (8), k4 (4) out: 37.44
+    "rhs": 16.0 + STATIC_B,                  # FP64 in and out (rhs callers): 18.24
+    "stage": 8 + 4 + STATIC_B + 4,           # u (8), k (4) in; k_out (4): 18.24
+    "fsal": 8 + 3 * 4 + STATIC_B + 8 + 4,    # u, k1..k3 in; uNew (8), k4 (4) out: 34.24
 }
 
 

@@ -339,6 +339,16 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
     b.HfYEnd.assign(5 * (size_t)d->Nx, 0.0);
     if (d->HfaceXEnd) b.HfXEnd.assign(d->HfaceXEnd, d->HfaceXEnd + 5 * d->Ny);
     if (d->HfaceYEnd) b.HfYEnd.assign(d->HfaceYEnd, d->HfaceYEnd + 5 * d->Nx);
+    // the kernels form dH/dx, dH/dy from Hnod as SGN2D does; given arrays must agree
+    std::vector<double> gx(c->Nd), gy(c->Nd);
+    depth_gradients(c->mesh, c->tab, b.Hnod.data(), gx.data(), gy.data());
+    if (std::memcmp(gx.data(), b.Hx.data(), c->Nd * sizeof(double)) != 0 ||
+        std::memcmp(gy.data(), b.Hy.data(), c->Nd * sizeof(double)) != 0) {
+      c->err = "SGNB_BATHY_ARRAYS: Hx, Hy must be the element-local GLL derivative of Hnod "
+               "over the Jacobian, as SGN2D computes them (src/solver/sgn2d.cpp:54-71)";
+      g_create_error = c->err;
+      return bail(SGNB_ERR_UNSUPPORTED);
+    }
   } else {
     bathymetry(c->mesh, c->tab, d->bathy_kind, d->bathy_par, b);
   }

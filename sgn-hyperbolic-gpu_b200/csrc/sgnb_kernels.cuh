@@ -69,9 +69,7 @@ struct Tile {
   static constexpr int NFIT = (NFACE + NTHR - 1) / NTHR;        // face-depth items per thread
   struct Smem {
     double U[NV][TE][NPP];       // tile state (input of R)
-    double H[TE][NPP];           // nodal still depth
-    double Hx[TE][NPP];          // nodal dH/dx
-    double Hy[TE][NPP];          // nodal dH/dy
+    double H[TE][NPP];           // nodal still depth (its gradient is formed from it)
     double G[NV + 1][TE][NPP];   // column-pass results dG (5 fields) and By; then dU
     // halo node states, flat index q = t + NP * (slot + NHALO * v):
     //   slot 0..TY-1        node (4,t) of the element left of tile row slot
@@ -93,6 +91,12 @@ struct Tile {
     return S.halo[t + NP * (slot + NHALO * v)];
   }
 };
+
+// Resident CTAs per SM the fast-mode single-instance kernels are compiled for (the
+// register budget per thread follows: 2 -> 168 registers, 3 -> 128).
+#ifndef SGNB_FAST_MIN_CTAS
+#define SGNB_FAST_MIN_CTAS 2
+#endif
 
 // Asynchronous global -> shared copy of one double (cp.async, no register staging), and
 // the wait for all of this thread's outstanding copies.
@@ -353,6 +357,30 @@ __device__ __forceinline__ void line_pass(const TC& C, const TB& Tb, const doubl
   }
 }
 
+// Nodal still-depth gradient at node (a, b) of one element from its nodal depths He:
+// the element-local GLL derivative over the Jacobian, dH/dx (DIR 0) or dH/dy (DIR 1), as
+// the solver's set-up defines it (src/solver/sgn2d.cpp:54-71). The exact mode repeats the
+// set-up's operation order (sum from 0.0, then a division), so it reproduces the
+// precomputed arrays bit for bit; reading them would cost 3.2 bytes per DOF.
+template <bool EXACT, int DIR, class TC, class TB>
+__device__ __forceinline__ double depth_grad(const TC& C, const TB& Tb, const double* He, int a,
+                                             int b) {
+  const int m = DIR == 0 ? a : b;
+  if constexpr (EXACT) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+      s += Tb.D[m * NP + k] * He[DIR == 0 ? k + NP * b : a + NP * k];
+    return s / (DIR == 0 ? C.Jx : C.Jy);
+  } else {
+    double s = Tb.D[m * NP] * He[DIR == 0 ? NP * b : a];
+#pragma unroll
+    for (int k = 1; k < NP; ++k)
+      s = fma(Tb.D[m * NP + k], He[DIR == 0 ? k + NP * b : a + NP * k], s);
+    return s * (DIR == 0 ? C.iJx : C.iJy);
+  }
+}
+
 // Mirror ghost across a wall normal to DIR: the normal discharge changes sign.
 template <int DIR>
 __device__ __forceinline__ void mirror(const double* own, double* ghost) {
@@ -435,8 +463,6 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
         cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
-        cp_async8(&(&S.Hx[0][0])[sof[u]], C.Hx + gof[u]);
-        cp_async8(&(&S.Hy[0][0])[sof[u]], C.Hy + gof[u]);
       }
     if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) {
       const double* __restrict__ src = MODE == MODE_RHS ? I.in : I.u;
@@ -672,10 +698,12 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             res = EXACT ? (-d - g) + S3 : S3 - (d + g);
           } else if (v == 1 || v == 2) {
             const double bath = C.g * (Un[a][0] - Hn[a]) + C.gamma * q.p;
-            const double Sv = bath * (v == 1 ? S.Hx[i][loc] : S.Hy[i][loc]);
+            const double Sv = bath * (v == 1 ? depth_grad<EXACT, 0>(C, Tb, S.H[i], a, j)
+                                             : depth_grad<EXACT, 1>(C, Tb, S.H[i], a, j));
             res = EXACT ? (-d - g) + Sv : Sv - (d + g);
           } else {
-            const double Hxl = S.Hx[i][loc], Hyl = S.Hy[i][loc];
+            const double Hxl = depth_grad<EXACT, 0>(C, Tb, S.H[i], a, j);
+            const double Hyl = depth_grad<EXACT, 1>(C, Tb, S.H[i], a, j);
             const double S4 = C.m2c2 * (q.w + q.u * Hxl + q.v * Hyl);
             const double Bx = C.mc2 * q.u * dhx[a];  // ncpX (sgn_flux2d.h:150-155)
             const double By = S.G[NV][i][loc];
@@ -792,7 +820,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 
 
 template <int MODE, bool EXACT>
-__global__ void __launch_bounds__(NTHR, 2) k_fused(const RhsConsts C, const StageArgs A) {
+__global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using T = Tile<8, 4>;
   T::Smem& S = *reinterpret_cast<T::Smem*>(smem_raw);

@@ -42,9 +42,7 @@ enum : int { MODE_RHS = 0, MODE_STAGE = 1, MODE_FSAL = 2 };
 
 struct Smem {
   double h[TE][NPP];          // full depth (FP64)
-  double H[TE][NPP];          // nodal still depth
-  double Hx[TE][NPP];
-  double Hy[TE][NPP];
+  double H[TE][NPP];          // nodal still depth (its gradient is formed from it)
   float q[4][TE][NPP];        // hu, hv, hw, hp (FP32 deviations)
   float G[NV + 1][TE][NPP];   // column-pass results (dG incl. the y hydrostatic part, By)
   double hhalo[NHALO * NP];   // halo depth, slot layout of sgnb_kernels.cuh
@@ -87,6 +85,18 @@ __device__ __forceinline__ double stage_value(const StageInM& I, long long idx) 
     return I.u[idx] + I.dt * (2.0 / 9.0 * (double)I.k1[idx] + 1.0 / 3.0 * (double)I.k2[idx] +
                               4.0 / 9.0 * (double)I.k3[idx]);
   }
+}
+
+// Nodal still-depth gradient at node (a, b) of an element from its nodal depths He (FP64):
+// the element-local GLL derivative over the Jacobian (src/solver/sgn2d.cpp:54-71), formed
+// from the depth tile instead of read from the precomputed arrays.
+template <int DIR>
+__device__ __forceinline__ double depth_grad(const RhsConsts& C, const double* He, int a, int b) {
+  const int m = DIR == 0 ? a : b;
+  double s = C.D[m * NP] * He[DIR == 0 ? NP * b : a];
+#pragma unroll
+  for (int k = 1; k < NP; ++k) s = fma(C.D[m * NP + k], He[DIR == 0 ? k + NP * b : a + NP * k], s);
+  return s * (DIR == 0 ? C.iJx : C.iJy);
 }
 
 // One point as seen by the FP32 part.
@@ -267,8 +277,6 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
         cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
-        cp_async8(&(&S.Hx[0][0])[sof[u]], C.Hx + gof[u]);
-        cp_async8(&(&S.Hy[0][0])[sof[u]], C.Hy + gof[u]);
       }
     double* __restrict__ unew = A.U[cur ^ 1];
     if constexpr (MODE == MODE_STAGE) {
@@ -444,7 +452,7 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
         C, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
         [&](int b, float deta, double dhyd, const PtF& s, float) {
           const int loc = j + NP * b;
-          const double Hyl = S.Hy[i][loc];
+          const double Hyl = depth_grad<1>(C, S.H[i], j, b);
           // ncpY with h_y = D eta + H_y (sgn_flux2d.h:156-161)
           S.G[NV][i][loc] = mc2f * s.v * (deta + (float)Hyl);
           // y hydrostatic part of dU[HV]: -d_y hyd + g (h - H) H_y, cancelled in FP64
@@ -482,14 +490,14 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
     } else halo_node(TY + iy, j, nhHi, nqHi);
     const double HfLo = hf_x(S, i, j);
     const double HfHi = (ix + 1 < TXv) ? hf_x(S, i + 1, j) : hf_xr(S, iy, j);
-    float hydu[NP], Bx[NP];
+    float hydu[NP], Bx[NP], Hxf[NP];
     line_mixed<0>(
         C, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
         [&](int a, float deta, double dhyd, const PtF& s, float) {
-          const int loc = a + NP * j;
-          const double Hxl = S.Hx[i][loc];
+          const double Hxl = depth_grad<0>(C, S.H[i], a, j);
           Bx[a] = mc2f * s.u * (deta + (float)Hxl);  // ncpX
           hydu[a] = (float)(C.g * (h[a] - Hn[a]) * Hxl - dhyd);
+          Hxf[a] = (float)Hxl;
         },
         [&](int a, int v, float d, const PtF& s) {
           const int loc = a + NP * j;
@@ -498,13 +506,13 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
           if (v == 0) {
             res = -(d + g);
           } else if (v == 1) {
-            res = hydu[a] + gammaf * s.p * (float)S.Hx[i][loc] - (d + g);
+            res = hydu[a] + gammaf * s.p * Hxf[a] - (d + g);
           } else if (v == 2) {
-            res = gammaf * s.p * (float)S.Hy[i][loc] - (d + g);
+            res = gammaf * s.p * (float)depth_grad<1>(C, S.H[i], a, j) - (d + g);
           } else if (v == 3) {
             res = gammaf * s.p - (d + g);
           } else {
-            const float Hxl = (float)S.Hx[i][loc], Hyl = (float)S.Hy[i][loc];
+            const float Hxl = Hxf[a], Hyl = (float)depth_grad<1>(C, S.H[i], a, j);
             const float S4 = (float)C.m2c2 * (s.w + s.u * Hxl + s.v * Hyl);
             res = S4 - (d + g) - Bx[a] - S.G[NV][i][loc];
           }

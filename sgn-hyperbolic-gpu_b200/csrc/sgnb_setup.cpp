@@ -177,6 +177,27 @@ void node_coords(const Mesh& m, const FrTables& t, double* x, double* y) {
   }
 }
 
+void depth_gradients(const Mesh& m, const FrTables& t, const double* Hnod, double* Hx,
+                     double* Hy) {
+  // nodal gradients: the GLL derivative of H along each x-line and y-line, over J
+  const int np = t.P + 1, npp = np * np;
+  const long long ne = (long long)m.Nx * m.Ny;
+  const double Jx = 0.5 * m.hx, Jy = 0.5 * m.hy;
+  for (long long e = 0; e < ne; ++e) {
+    const double* He = Hnod + e * npp;
+    for (int b = 0; b < np; ++b)
+      for (int a = 0; a < np; ++a) {
+        double sx = 0.0, sy = 0.0;
+        for (int k = 0; k < np; ++k) {
+          sx += t.D[a * np + k] * He[k + np * b];
+          sy += t.D[b * np + k] * He[a + np * k];
+        }
+        Hx[e * npp + a + np * b] = sx / Jx;
+        Hy[e * npp + a + np * b] = sy / Jy;
+      }
+  }
+}
+
 void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p,
                 Bathymetry& out) {
   const int np = t.P + 1, npp = np * np;
@@ -192,21 +213,7 @@ void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p,
   std::vector<double> x(Nd), y(Nd);
   node_coords(m, t, x.data(), y.data());
   for (long long i = 0; i < Nd; ++i) out.Hnod[i] = still_depth(kind, p, x[i], y[i]);
-  // nodal gradients: the GLL derivative of H along each x-line and y-line, over J
-  const double Jx = 0.5 * m.hx, Jy = 0.5 * m.hy;
-  for (long long e = 0; e < ne; ++e) {
-    const double* He = out.Hnod.data() + e * npp;
-    for (int b = 0; b < np; ++b)
-      for (int a = 0; a < np; ++a) {
-        double sx = 0.0, sy = 0.0;
-        for (int k = 0; k < np; ++k) {
-          sx += t.D[a * np + k] * He[k + np * b];
-          sy += t.D[b * np + k] * He[a + np * k];
-        }
-        out.Hx[e * npp + a + np * b] = sx / Jx;
-        out.Hy[e * npp + a + np * b] = sy / Jy;
-      }
-  }
+  depth_gradients(m, t, out.Hnod.data(), out.Hx.data(), out.Hy.data());
   // face depths sampled on the left / bottom element edges at the transverse nodes
   for (long long e = 0; e < ne; ++e) {
     const int ex = (int)(e % m.Nx), ey = (int)(e / m.Nx);

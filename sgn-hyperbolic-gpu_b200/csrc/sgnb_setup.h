@@ -29,6 +29,11 @@ double still_depth(int kind, const double* p, double x, double y);
 int bathy_param_count(int kind, const double* p, int n);
 void node_coords(const Mesh& m, const FrTables& t, double* x, double* y);
 void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p, Bathymetry& out);
+// Nodal dH/dx, dH/dy: the element-local GLL derivative of the nodal depth over the
+// Jacobian (src/solver/sgn2d.cpp:54-71); the fused kernels form the same values from the
+// depth tile instead of reading them.
+void depth_gradients(const Mesh& m, const FrTables& t, const double* Hnod, double* Hx,
+                     double* Hy);
 // Transpose of bathymetry() for kind 5 (cell means p = {Mx, My, Lx, Ly, means...}):
 // cotangents of every static (bar) -> cotangent of the Mx * My means.
 void cells_transpose(const Mesh& m, const FrTables& t, const double* p, const Bathymetry& bar,

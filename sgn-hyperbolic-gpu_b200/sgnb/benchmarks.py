@@ -7,9 +7,10 @@ sweep    configuration 4: 256 instances (workloads.cfg4_instances) advanced K ac
          steps each by the batched launches (after the autotuner), against the same
          instances run one after another through the single-instance device loop.
 mixed    configuration 2 in FP64 (fast) and in the mixed-precision mode, K steps each,
-         and the free-surface error of the mixed run: both replay the FP64 run's accepted
-         step sizes from the same state; eta L2 (RMS over the nodes) and Linf of the
-         difference.
+         and the free-surface error of the mixed mode against FP64: every mode replays
+         two step sequences from the same state (constant 0.8 x the CFL-0.5 step, and the
+         FP64 run's accepted steps), with FP64 fast against FP64 exact as the control;
+         eta L2 (RMS over the nodes) and Linf of the differences.
 adjoint  configuration 5: the frozen 200-step trajectory with 16 gauges (forward), its
          vector-Jacobian product (checkpoint-and-recompute every 20 steps), and one
          central-difference check of a directional derivative.
@@ -22,13 +23,15 @@ import time
 
 import numpy as np
 
-from . import FP64_FAST, MIXED, SGN2DB200, SGNBatch
+from . import FP64_FAST, MIXED, SGN2DB200, SGNBatch, SgnbError
 from . import workloads as W
 
 METRIC = "DOF-updates/s per RK stage"
 UNIT = "DOF-updates/s"
-STAGE_LOOP_BYTES = 112.32  # FP64 fused BS3(2) attempt, algorithmic bytes per DOF
-MIXED_LOOP_BYTES = 2 * 21.44 + 37.44
+# algorithmic bytes per DOF of one fused BS3(2) attempt (two intermediate stages and the
+# end-point stage; nodal depth gradients formed on chip): FP64 and mixed precision
+STAGE_LOOP_BYTES = 2 * 26.24 + 50.24
+MIXED_LOOP_BYTES = 2 * 18.24 + 34.24
 
 
 def _events(torch, stream=None):
@@ -120,6 +123,8 @@ def run_sweep(args, clock_sampler, peak):
 def run_mixed(args, clock_sampler, peak):
     import torch
 
+    from . import FP64_EXACT
+
     Nx, Ny = W.CFG2["Nx"], W.CFG2["Ny"]
     if args.mesh:
         Nx, Ny = args.mesh
@@ -127,39 +132,60 @@ def run_mixed(args, clock_sampler, peak):
     dof = 125.0 * Nx * Ny
     Ud = W.cfg2_state_torch(Nx, Ny)
     res = {}
-    dts = None
-    finals = {}
+    seqs = {}
+    finals = {"adaptive": {}, "stable": {}}
     clocks = None
-    for name, prec in (("fp64", FP64_FAST), ("mixed", MIXED)):
+    for name, prec in (("fp64", FP64_FAST), ("mixed", MIXED), ("exact", FP64_EXACT)):
         with SGN2DB200(precision=prec, **kw) as d:
             d.upload_tensor(Ud)
             dt0 = d.cfl_time_step(0.5)
-            d.integrate_steps(0.0, dt0, args.warmup)
-            d.upload_tensor(Ud)
-            _, sp = d.state_device_ptr()
-            stream = torch.cuda.ExternalStream(sp)
-            e0, e1 = _events(torch, stream)
-            torch.cuda.synchronize()
-            with clock_sampler(0) as clk:
-                e0.record(stream)
-                st = d.integrate_steps(0.0, dt0, args.steps)
-                e1.record(stream)
+            if name != "exact":
+                d.integrate_steps(0.0, dt0, args.warmup)
+                d.upload_tensor(Ud)
+                _, sp = d.state_device_ptr()
+                stream = torch.cuda.ExternalStream(sp)
+                e0, e1 = _events(torch, stream)
                 torch.cuda.synchronize()
-            t = e0.elapsed_time(e1) / 1e3
-            res[name] = dict(value=dof * st.rhsEvals / t, time_s=t, accepted=st.accepted,
-                             rejected=st.rejected, launches=st.kernel_launches)
-            if name == "mixed":
-                clocks = clk.summary()
+                with clock_sampler(0) as clk:
+                    e0.record(stream)
+                    st = d.integrate_steps(0.0, dt0, args.steps)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / 1e3
+                res[name] = dict(value=dof * st.rhsEvals / t, time_s=t, accepted=st.accepted,
+                                 rejected=st.rejected, launches=st.kernel_launches)
+                if name == "mixed":
+                    clocks = clk.summary()
             if name == "fp64":
                 log = d.attempt_log()
-                dts = log[log[:, 3] == 1][:, 1].copy()
-            # eta after replaying the FP64 run's accepted steps from the same state
-            d.upload_tensor(Ud)
-            d.bs3_steps(0.0, dts)
-            finals[name] = d.state_tensor()[: d.Nd].clone()  # h; eta differences = h differences
-    diff = (finals["mixed"] - finals["fp64"]).double()
-    eta_l2 = float(torch.sqrt(torch.mean(diff * diff)))
-    eta_linf = float(diff.abs().max())
+                seqs["adaptive"] = log[log[:, 3] == 1][:, 1].copy()
+                seqs["stable"] = np.full(len(seqs["adaptive"]), 0.8 * dt0)
+            # free surface after each step sequence, from the same state
+            for key, dts in seqs.items():
+                d.upload_tensor(Ud)
+                try:
+                    d.bs3_steps(0.0, dts)
+                    finals[key][name] = d.state_tensor()[: d.Nd].clone()  # h
+                except SgnbError:  # the replay left the stable range (non-finite state)
+                    finals[key][name] = None
+
+    def err(key, a, b):
+        if finals[key][a] is None or finals[key][b] is None:
+            return {"diverged": [n for n in (a, b) if finals[key][n] is None]}
+        diff = (finals[key][a] - finals[key][b]).double()  # eta differences = h differences
+        return {"l2_rms": float(torch.sqrt(torch.mean(diff * diff))),
+                "linf": float(diff.abs().max())}
+
+    errors = {
+        "stable_steps": {"mixed_vs_fp64": err("stable", "mixed", "fp64"),
+                         "fp64_fast_vs_exact": err("stable", "fp64", "exact"),
+                         "steps": "constant 0.8 x the CFL-0.5 step"},
+        "adaptive_steps": {"mixed_vs_fp64": err("adaptive", "mixed", "fp64"),
+                           "fp64_fast_vs_exact": err("adaptive", "fp64", "exact"),
+                           "steps": "the FP64 run's accepted step sizes (near the stability "
+                                    "limit: round-off of any kind is amplified)"},
+        "how": "each mode replays the step sequence from the same state (bs3 steps)",
+    }
     ratio = res["mixed"]["value"] / res["fp64"]["value"]
     achieved = MIXED_LOOP_BYTES * res["mixed"]["value"] / 3.0 / 1e9  # bytes per attempt
     line = {
@@ -171,10 +197,7 @@ def run_mixed(args, clock_sampler, peak):
         "config": {"workload": f"configuration 2 ({Nx}x{Ny}, {int(dof):,} DOF), mixed "
                                "precision against FP64 (fast)", "mesh": [Nx, Ny]},
         "fp64": res["fp64"], "mixed": res["mixed"], "speedup_vs_fp64": ratio,
-        "eta_error_vs_fp64": {"l2_rms": eta_l2, "linf": eta_linf,
-                              "steps": int(len(dts)),
-                              "how": "both modes replay the FP64 run's accepted step sizes "
-                                     "from the same state; eta difference = h difference"},
+        "eta_error": errors,
         "roofline": {"bound": "hbm", "kernel": "mixed stage loop (average over an attempt)",
                      "achieved": round(achieved, 1), "peak": peak[0], "peak_kind": peak[1],
                      "unit": "GB/s", "frac": round(achieved / peak[0], 4), "traffic": None},

@@ -176,13 +176,21 @@ def smooth_random_field(x, y, Lx, Ly, rng, n=12, kmax=4):
     return f / np.sqrt(n)
 
 
-def fd_sweep(loss_of, p0, d, adj, steps=(1.0, 1e-1, 1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7)):
-    """Relative errors of central differences along d for a sweep of steps."""
+def fd_sweep(loss_of, p0, d, adj, h0=0.4, n=19):
+    """Relative errors of central differences along d over steps h0 / 2^k, k < n: the
+    second-order stencil D2(h) = (L(p + h d) - L(p - h d)) / 2h and the fourth-order
+    central stencil (4 D2(h) - D2(2h)) / 3."""
     errs = []
-    for eps in steps:
-        fd = (loss_of(*(a + eps * b for a, b in zip(p0, d))) -
+    prev = None
+    for k in range(n):
+        eps = h0 / 2 ** k
+        d2 = (loss_of(*(a + eps * b for a, b in zip(p0, d))) -
               loss_of(*(a - eps * b for a, b in zip(p0, d)))) / (2 * eps)
-        errs.append(abs(fd - adj) / max(abs(fd), abs(adj)))
+        errs.append(abs(d2 - adj) / max(abs(d2), abs(adj)))
+        if prev is not None:
+            d4 = (4.0 * d2 - prev) / 3.0
+            errs.append(abs(d4 - adj) / max(abs(d4), abs(adj)))
+        prev = d2
     return errs
 
 
@@ -194,9 +202,9 @@ def test_config5_gradients():
     1.2 x the CFL-0.5 step, where grid-scale perturbations of the free surface grow: along
     the uncapped sequence finite differences of white noise in eta0 leave the linear
     range for steps above 1e-6, whatever the adjoint. The loss depends weakly on the
-    bathymetry over 200 steps (directional derivatives of order 1e-11), so its central
-    differences are rounding-limited below steps of 1e-2 and the sweep reaches up to 1
-    (a depth change of 1 % at most)."""
+    bathymetry over 200 steps (directional derivatives of order 1e-11): second-order
+    central differences are rounding-limited below steps of 1e-2 and truncation-limited
+    above, so the sweep also forms the fourth-order central stencil."""
     P = W.cfg5_problem()
     kw = P["kw"]
     cfg = W.CFG5
@@ -234,4 +242,5 @@ def test_config5_gradients():
                 for k, dv in enumerate(dirs):
                     adj = float(gm @ dv[0] + ge @ dv[1])
                     errs = fd_sweep(loss_of, p0, dv, adj)
-                    assert min(errs) <= 1e-6, f"{label} direction {k}: relative errors {errs}"
+                    # large steps of white noise overflow (NaN): the sweep keeps the rest
+                    assert np.nanmin(errs) <= 1e-6, f"{label} direction {k}: errors {errs}"
