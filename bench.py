@@ -169,6 +169,8 @@ def run_ours(args):
     if args.mesh:
         Nx, Ny = args.mesh
     kw = W.cfg2_solver_args(Nx, Ny, Lx, Ly)
+    if args.bc == "periodic":
+        kw.update(bc_x=0, bc_y=0)
     prec = {"fast": sgnb.FP64_FAST, "exact": sgnb.FP64_EXACT, "mixed": sgnb.MIXED}[args.precision]
     dof = 5 * 25 * Nx * Ny
     Ud = W.cfg2_state_torch(Nx, Ny, Lx, Ly, device=f"cuda:{local}")
@@ -271,8 +273,8 @@ def run_ours(args):
             "dtype": "f64 state, f32 deviations" if args.precision == "mixed" else "f64",
             "data": "synthetic",
             "config": {"workload": f"configuration 2: {Nx}x{Ny} P=4 ({dof:,} DOF), "
-                                   "40x20 basin with reflective walls, elliptic shoal, "
-                                   "8 random-phase sines; adaptive BS3(2) steps",
+                                   f"40x20 basin with {'reflective walls' if args.bc == 'walls' else 'periodic boundaries'}, "
+                                   "elliptic shoal, 8 random-phase sines; adaptive BS3(2) steps",
                        "mesh": [Nx, Ny], "dof": dof, "precision": f"fp64-{args.precision}",
                        "accepted": st.accepted, "rejected": st.rejected,
                        "rhs_evals": st.rhsEvals, "l2": "inputs larger than L2 "
@@ -344,10 +346,49 @@ def _ref_worker(args):
     return time.perf_counter() - t0, 5 * o.Nd
 
 
+def run_reference_gpu(args):
+    """The reference's single-GPU solver (SGN2DCuda::integrateAdaptive, compiled from its
+    sources by oracle/Makefile) on configuration 2 with periodic boundaries."""
+    from sgnb import workloads as W
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_bench")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_gpu_bench not "
+                          "built (make -C oracle refgpu needs the reference sources)"}))
+        return
+    Nx, Ny, Lx, Ly = W.CFG2["Nx"], W.CFG2["Ny"], W.CFG2["Lx"], W.CFG2["Ly"]
+    if args.mesh:
+        Nx, Ny = args.mesh
+    shoal, waves = W.cfg2_params()
+    argv = [exe, str(Nx), str(Ny), repr(Lx), repr(Ly), str(args.steps), "1"]
+    argv += [repr(float(v)) for v in shoal]
+    for arr in waves:
+        argv += [repr(float(v)) for v in arr]
+    with ClockSampler(0) as clk:
+        out = subprocess.run(argv, check=True, capture_output=True, text=True).stdout
+    r = json.loads(out.strip().splitlines()[-1])
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
+        "n_gpus": 1, "steps": int(r["accepted"]), "warmup": 1,
+        "ms_per_step": r["time_s"] / max(r["accepted"], 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"configuration 2 mesh ({Nx}x{Ny} P=4), periodic boundaries, "
+                               "the reference's single-GPU solver SGN2DCuda::integrateAdaptive "
+                               f"over [0, {args.steps} x dt_CFL0.5]", "reference": r},
+        "clocks": clk.summary(),
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return  # under torchrun the other ranks exit without work
+    if args.ref_device == "gpu":
+        run_reference_gpu(args)
+        return
     import multiprocessing as mp
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -398,6 +439,13 @@ def main():
                          "FP64 on configuration 2 with the eta error; adjoint: "
                          "configuration 5 forward + VJP")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bc", choices=["walls", "periodic"], default="walls",
+                    help="boundaries of configuration 2 (periodic: the reference solver's "
+                         "only kind, for the comparison with --ref-device gpu)")
+    ap.add_argument("--ref-device", choices=["cpu", "gpu"], default="cpu",
+                    help="reference arm: the reference's CPU solver (default) or its "
+                         "single-GPU solver SGN2DCuda (oracle/_ref/ref_gpu_bench) on "
+                         "configuration 2 with periodic boundaries")
     ap.add_argument("--mesh", type=int, nargs=2, metavar=("NX", "NY"), default=None,
                     help="smaller mesh of the same workload, for profiler captures only")
     args = ap.parse_args()

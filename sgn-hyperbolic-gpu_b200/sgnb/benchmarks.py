@@ -8,7 +8,7 @@ sweep    configuration 4: 256 instances (workloads.cfg4_instances) advanced K ac
          instances run one after another through the single-instance device loop.
 mixed    configuration 2 in FP64 (fast) and in the mixed-precision mode, K steps each,
          and the free-surface error of the mixed mode against FP64: every mode replays
-         two step sequences from the same state (constant 0.8 x the CFL-0.5 step, and the
+         two step sequences from the same state (constant 0.4 x the CFL-0.5 step, and the
          FP64 run's accepted steps), with FP64 fast against FP64 exact as the control;
          eta L2 (RMS over the nodes) and Linf of the differences.
 adjoint  configuration 5: the frozen 200-step trajectory with 16 gauges (forward), its
@@ -159,7 +159,7 @@ def run_mixed(args, clock_sampler, peak):
             if name == "fp64":
                 log = d.attempt_log()
                 seqs["adaptive"] = log[log[:, 3] == 1][:, 1].copy()
-                seqs["stable"] = np.full(len(seqs["adaptive"]), 0.8 * dt0)
+                seqs["stable"] = np.full(len(seqs["adaptive"]), 0.4 * dt0)
             # free surface after each step sequence, from the same state
             for key, dts in seqs.items():
                 d.upload_tensor(Ud)
@@ -179,7 +179,7 @@ def run_mixed(args, clock_sampler, peak):
     errors = {
         "stable_steps": {"mixed_vs_fp64": err("stable", "mixed", "fp64"),
                          "fp64_fast_vs_exact": err("stable", "fp64", "exact"),
-                         "steps": "constant 0.8 x the CFL-0.5 step"},
+                         "steps": "constant 0.4 x the CFL-0.5 step"},
         "adaptive_steps": {"mixed_vs_fp64": err("adaptive", "mixed", "fp64"),
                            "fp64_fast_vs_exact": err("adaptive", "fp64", "exact"),
                            "steps": "the FP64 run's accepted step sizes (near the stability "
