@@ -200,10 +200,11 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
 
 /* Batched sweep (no reference counterpart; the reference runs one instance per
  * SGN2DCuda): n independent instances (their own mesh size, parameters, bathymetry and
- * state; SGNB_FP64_FAST) advanced together, one persistent launch per RK stage over all
- * instances' tiles, each instance with its own adaptive controller, attempts replayed
- * as CUDA-graph chunks. Instance i is an ordinary context (sgnb_batch_instance) for
- * upload / download / diagnostics between runs. */
+ * state) advanced together, one launch per RK stage over all instances' tiles, each
+ * instance with its own adaptive controller, attempts replayed as CUDA-graph chunks. All
+ * instances of a batch run in one arithmetic mode: SGNB_FP64_FAST (tile shapes 8x4, 16x2,
+ * 4x8) or SGNB_MIXED (8x4 tiles). Instance i is an ordinary context
+ * (sgnb_batch_instance) for upload / download / diagnostics between runs. */
 typedef struct sgnb_batch sgnb_batch;
 int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out);
 int sgnb_batch_destroy(sgnb_batch* b);
@@ -223,8 +224,8 @@ int sgnb_batch_get_config(const sgnb_batch* b, int* shape, int* blocks);
 /* Autotuner: times one adaptive attempt (three stage launches, reps times) for every tile
  * shape and grid (one CTA per tile, persistent grids of 1..4 CTAs per SM) at step sizes
  * dt0[i], keeps the fastest (sgnb_batch_get_config reports it). ms_out (optional, 15
- * entries, shape-major) receives the measured ms per attempt. The instances' states are
- * left unchanged. */
+ * entries, shape-major) receives the measured ms per attempt (-1 for shapes a mixed batch
+ * does not use). The instances' states are left unchanged. */
 int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_out);
 const char* sgnb_batch_last_error(const sgnb_batch* b);
 

@@ -325,6 +325,7 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   if (e == cudaSuccess) e = dev::prepare_fused_fast();
   if (e == cudaSuccess) e = dev::prepare_fused_mixed();
   if (e == cudaSuccess) e = dev::prepare_fused_batch();
+  if (e == cudaSuccess) e = dev::prepare_mixed_batch();
   if (e != cudaSuccess) { cuda_fail(c, e, "kernel attributes"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
 
   // statics: Hnod, Hx, Hy (Nd each), HfX, HfY (5 ne each), HfXEnd (5 Ny), HfYEnd (5 Nx)
@@ -658,8 +659,11 @@ struct sgnb_batch {
   cudaStream_t stream = nullptr;
   std::vector<sgnb_ctx*> ctx;          // per-instance buffers and statics
   RhsConsts* dconsts = nullptr;        // [n]
+  bool mixed = false;                  // every instance SGNB_MIXED (else SGNB_FP64_FAST)
   StageArgs* dargs = nullptr;          // [n]
   StageArgs* hargs = nullptr;          // pinned host mirror
+  StageArgsM* dargsM = nullptr;        // [n], mixed batches
+  StageArgsM* hargsM = nullptr;
   CtrlState* dctrl = nullptr;          // [n]
   CtrlState* hctrl = nullptr;          // pinned host mirror
   double* dpartbuf = nullptr;          // error partials of every instance, 3 per tile
@@ -694,6 +698,9 @@ int bfail(sgnb_batch* b, int code, const std::string& msg) {
                    std::string(#call) + ": " + cudaGetErrorName(e_));       \
   } while (0)
 
+// One batched stage launch of either arithmetic mode.
+cudaError_t batch_launch(sgnb_batch* b, int mode, int shape, int blocks, int kin_k2, double coef);
+
 BatchArgs batch_args(sgnb_batch* b, int shape, int kin_k2, double coef) {
   BatchArgs B{};
   const RhsConsts& C0 = b->ctx[0]->C;
@@ -716,11 +723,9 @@ int batch_build_graph(sgnb_batch* b, int len) {
   SGNB_BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < len && e == cudaSuccess; ++k) {
-    e = dev::launch_fused_batch(1, b->shape, b->blocks, batch_args(b, b->shape, 0, 0.5), b->stream);
-    if (e == cudaSuccess)
-      e = dev::launch_fused_batch(1, b->shape, b->blocks, batch_args(b, b->shape, 1, 0.75), b->stream);
-    if (e == cudaSuccess)
-      e = dev::launch_fused_batch(2, b->shape, b->blocks, batch_args(b, b->shape, 0, 0.0), b->stream);
+    e = batch_launch(b, 1, b->shape, b->blocks, 0, 0.5);
+    if (e == cudaSuccess) e = batch_launch(b, 1, b->shape, b->blocks, 1, 0.75);
+    if (e == cudaSuccess) e = batch_launch(b, 2, b->shape, b->blocks, 0, 0.0);
     if (e == cudaSuccess)
       e = dev::launch_controller_batch(b->dctrl, b->dpart, b->dnblk[b->shape], b->dntot, b->n,
                                        b->stream);
@@ -744,7 +749,41 @@ bool all_done(const sgnb_batch* b) {
 
 // Stage arguments of every instance and the controllers (already initialised in
 // b->hctrl) to the device.
+cudaError_t batch_launch(sgnb_batch* b, int mode, int shape, int blocks, int kin_k2, double coef) {
+  if (!b->mixed) return dev::launch_fused_batch(mode, shape, blocks, batch_args(b, shape, kin_k2, coef), b->stream);
+  if (shape != 0) return cudaErrorInvalidValue;  // mixed batches use 8x4 tiles
+  const BatchArgs B = batch_args(b, 0, kin_k2, coef);
+  BatchArgsM M{};
+  M.tables = B.tables;
+  M.consts = B.consts;
+  M.args = b->dargsM;
+  M.tile_inst = B.tile_inst;
+  M.tile_start = B.tile_start;
+  M.ntiles = B.ntiles;
+  M.kin_k2 = kin_k2;
+  M.coef = coef;
+  return dev::launch_mixed_batch(mode, blocks, M, b->stream);
+}
+
 int batch_prepare(sgnb_batch* b) {
+  if (b->mixed) {
+    for (int i = 0; i < b->n; ++i) {
+      sgnb_ctx* c = b->ctx[i];
+      StageArgsM& A = b->hargsM[i];
+      A = StageArgsM{};
+      A.U[0] = c->U[0]; A.U[1] = c->U[1];
+      A.K1[0] = (float*)c->K1[0]; A.K1[1] = (float*)c->K1[1];
+      A.K2 = (float*)c->K2; A.K3 = (float*)c->K3;
+      A.ctrl = b->dctrl + i;
+      A.partials = b->hpart[i];
+      A.in = c->U[c->cur];               // FSAL head: R(u) into K1[cur] (FP32)
+      A.outd = nullptr;
+      A.out = (float*)c->K1[c->cur];
+    }
+    SGNB_BCU(b, cudaMemcpyAsync(b->dargsM, b->hargsM, b->n * sizeof(StageArgsM), cudaMemcpyHostToDevice, b->stream));
+    SGNB_BCU(b, cudaMemcpyAsync(b->dctrl, b->hctrl, b->n * sizeof(CtrlState), cudaMemcpyHostToDevice, b->stream));
+    return SGNB_OK;
+  }
   for (int i = 0; i < b->n; ++i) {
     sgnb_ctx* c = b->ctx[i];
     StageArgs& A = b->hargs[i];
@@ -767,7 +806,7 @@ int batch_run(sgnb_batch* b) {
   const int len = 8;
   if (int rc = batch_build_graph(b, len)) return rc;
   if (int rc = batch_prepare(b)) return rc;
-  SGNB_BCU(b, dev::launch_fused_batch(0, b->shape, b->blocks, batch_args(b, b->shape, 0, 0.0), b->stream));
+  SGNB_BCU(b, batch_launch(b, 0, b->shape, b->blocks, 0, 0.0));
   b->launches = 1 + 4LL * len;
   SGNB_BCU(b, cudaGraphLaunch(b->chunk, b->stream));
   SGNB_BCU(b, cudaMemcpyAsync(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost, b->stream));
@@ -794,12 +833,15 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
   if (!out || !descs || n < 1) return bfail(nullptr, SGNB_ERR_INVALID, "descs, n >= 1, out");
   *out = nullptr;
   for (int i = 0; i < n; ++i) {
-    if (descs[i].precision != SGNB_FP64_FAST)
-      return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run in SGNB_FP64_FAST");
+    if (descs[i].precision != SGNB_FP64_FAST && descs[i].precision != SGNB_MIXED)
+      return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run in SGNB_FP64_FAST or SGNB_MIXED");
+    if (descs[i].precision != descs[0].precision)
+      return bfail(nullptr, SGNB_ERR_INVALID, "all instances of a batch in one arithmetic mode");
     if (descs[i].device != descs[0].device)
       return bfail(nullptr, SGNB_ERR_INVALID, "all instances on one device");
   }
   sgnb_batch* b = new sgnb_batch();
+  b->mixed = descs[0].precision == SGNB_MIXED;
   b->n = n;
   b->device = descs[0].device;
   b->ctx.assign(n, nullptr);
@@ -818,6 +860,8 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
   if (e == cudaSuccess) e = cudaMalloc(&b->dconsts, n * sizeof(RhsConsts));
   if (e == cudaSuccess) e = cudaMalloc(&b->dargs, n * sizeof(StageArgs));
   if (e == cudaSuccess) e = cudaMallocHost(&b->hargs, n * sizeof(StageArgs));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dargsM, n * sizeof(StageArgsM));
+  if (e == cudaSuccess) e = cudaMallocHost(&b->hargsM, n * sizeof(StageArgsM));
   if (e == cudaSuccess) e = cudaMalloc(&b->dctrl, n * sizeof(CtrlState));
   if (e == cudaSuccess) e = cudaMallocHost(&b->hctrl, n * sizeof(CtrlState));
   if (e == cudaSuccess) e = cudaMalloc(&b->dpart, n * sizeof(double*));
@@ -882,6 +926,8 @@ int sgnb_batch_destroy(sgnb_batch* b) {
   cudaFree(b->dconsts); cudaFree(b->dargs); cudaFree(b->dctrl); cudaFree(b->dpart);
   cudaFree(b->dntot); cudaFree(b->dpartbuf);
   if (b->hargs) cudaFreeHost(b->hargs);
+  cudaFree(b->dargsM);
+  if (b->hargsM) cudaFreeHost(b->hargsM);
   if (b->hctrl) cudaFreeHost(b->hctrl);
   for (int sh = 0; sh < 3; ++sh) {
     cudaFree(b->dtile_inst[sh]); cudaFree(b->dtile_start[sh]); cudaFree(b->dnblk[sh]);
@@ -906,6 +952,7 @@ sgnb_ctx* sgnb_batch_instance(sgnb_batch* b, int i) {
 
 int sgnb_batch_set_config(sgnb_batch* b, int shape, int blocks) {
   if (!b || shape < 0 || shape > 2 || blocks < 0) return bfail(b, SGNB_ERR_INVALID, "shape 0..2, blocks >= 0");
+  if (b->mixed && shape != 0) return bfail(b, SGNB_ERR_UNSUPPORTED, "mixed batches use 8x4 tiles");
   b->shape = shape;
   b->blocks = blocks;
   return SGNB_OK;
@@ -986,17 +1033,17 @@ int sgnb_batch_autotune(sgnb_batch* b, const double* dt0, int reps, double* ms_o
   double best = 1e300;
   int bestShape = 0, bestBlocks = 0;
   int rc = SGNB_OK;
-  for (int sh = 0; sh < 3 && rc == SGNB_OK; ++sh) {
+  if (ms_out)
+    for (int q = 0; q < 3 * kTuneGrids; ++q) ms_out[q] = -1.0;  // shapes not tried
+  for (int sh = 0; sh < (b->mixed ? 1 : 3) && rc == SGNB_OK; ++sh) {
     for (int f = 0; f < kTuneGrids && rc == SGNB_OK; ++f) {
       const int blocks = f * sms;
       auto run = [&](int count) {
         cudaError_t e = cudaSuccess;
         for (int r = 0; r < count && e == cudaSuccess; ++r) {
-          e = dev::launch_fused_batch(1, sh, blocks, batch_args(b, sh, 0, 0.5), b->stream);
-          if (e == cudaSuccess)
-            e = dev::launch_fused_batch(1, sh, blocks, batch_args(b, sh, 1, 0.75), b->stream);
-          if (e == cudaSuccess)
-            e = dev::launch_fused_batch(2, sh, blocks, batch_args(b, sh, 0, 0.0), b->stream);
+          e = batch_launch(b, 1, sh, blocks, 0, 0.5);
+          if (e == cudaSuccess) e = batch_launch(b, 1, sh, blocks, 1, 0.75);
+          if (e == cudaSuccess) e = batch_launch(b, 2, sh, blocks, 0, 0.0);
         }
         return e;
       };

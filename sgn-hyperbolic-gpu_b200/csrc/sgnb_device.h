@@ -136,7 +136,23 @@ struct GatherArgs {
   double* HfYEndacc;
 };
 
+// Work list of a batched mixed-precision launch (8x4 tiles), as BatchArgs.
+struct BatchArgsM {
+  FrTablesDev tables;
+  const RhsConsts* consts;
+  const StageArgsM* args;
+  const int* tile_inst;
+  const long long* tile_start;
+  long long ntiles;
+  int kin_k2;
+  double coef;
+};
+
 namespace dev {
+// Batched mixed-precision launch: `blocks` persistent CTAs, or one CTA per tile (0).
+cudaError_t launch_mixed_batch(int mode, int blocks, const BatchArgsM& B, cudaStream_t s);
+cudaError_t prepare_mixed_batch();
+
 // Adjoint kernels (FP64, fast arithmetic).
 cudaError_t launch_vjp_rhs(const RhsConsts& C, const FrTablesDev& T, const VjpArgs& A,
                            const GatherArgs& G, cudaStream_t s);

@@ -34,5 +34,42 @@ cudaError_t prepare_fused_mixed() {
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
+template <int MODE>
+static cudaError_t launch_mb(int blocks, const BatchArgsM& B, cudaStream_t s) {
+  if (blocks > 0) {
+    mix::k_mixed_batch<MODE, true><<<blocks, mix::NTHR, sizeof(mix::Smem), s>>>(B);
+  } else {
+    if (B.ntiles < 1 || B.ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    mix::k_mixed_batch<MODE, false><<<(unsigned)B.ntiles, mix::NTHR, sizeof(mix::Smem), s>>>(B);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_batch(int mode, int blocks, const BatchArgsM& B, cudaStream_t s) {
+  switch (mode) {
+    case 0: return launch_mb<mix::MODE_RHS>(blocks, B, s);
+    case 1: return launch_mb<mix::MODE_STAGE>(blocks, B, s);
+    case 2: return launch_mb<mix::MODE_FSAL>(blocks, B, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int MODE>
+static cudaError_t prepare_mb() {
+  const int bytes = (int)sizeof(mix::Smem);
+  cudaError_t e = cudaFuncSetAttribute(mix::k_mixed_batch<MODE, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(mix::k_mixed_batch<MODE, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t prepare_mixed_batch() {
+  cudaError_t e = prepare_mb<mix::MODE_RHS>();
+  if (e == cudaSuccess) e = prepare_mb<mix::MODE_STAGE>();
+  if (e == cudaSuccess) e = prepare_mb<mix::MODE_FSAL>();
+  return e;
+}
+
 }  // namespace dev
 }  // namespace sgnb

@@ -90,12 +90,13 @@ __device__ __forceinline__ double stage_value(const StageInM& I, long long idx) 
 // Nodal still-depth gradient at node (a, b) of an element from its nodal depths He (FP64):
 // the element-local GLL derivative over the Jacobian (src/solver/sgn2d.cpp:54-71), formed
 // from the depth tile instead of read from the precomputed arrays.
-template <int DIR>
-__device__ __forceinline__ double depth_grad(const RhsConsts& C, const double* He, int a, int b) {
+template <int DIR, class TC, class TB>
+__device__ __forceinline__ double depth_grad(const TC& C, const TB& Tb, const double* He, int a,
+                                             int b) {
   const int m = DIR == 0 ? a : b;
-  double s = C.D[m * NP] * He[DIR == 0 ? NP * b : a];
+  double s = Tb.D[m * NP] * He[DIR == 0 ? NP * b : a];
 #pragma unroll
-  for (int k = 1; k < NP; ++k) s = fma(C.D[m * NP + k], He[DIR == 0 ? k + NP * b : a + NP * k], s);
+  for (int k = 1; k < NP; ++k) s = fma(Tb.D[m * NP + k], He[DIR == 0 ? k + NP * b : a + NP * k], s);
   return s * (DIR == 0 ? C.iJx : C.iJy);
 }
 
@@ -117,8 +118,8 @@ __device__ __forceinline__ PtF make_pt(double h64, float hu, float hv, float hw,
 }
 
 // FP32 (deviation) part of flux field v; the hydrostatic term is added in FP64 elsewhere.
-template <int DIR>
-__device__ __forceinline__ float flux_dev(const RhsConsts& C, int v, const PtF& s) {
+template <int DIR, class TC>
+__device__ __forceinline__ float flux_dev(const TC& C, int v, const PtF& s) {
   switch (v) {
     case 0: return s.hn;
     case 1: return DIR == 0 ? s.hu * s.u + s.hp : s.hv * s.u;
@@ -128,15 +129,16 @@ __device__ __forceinline__ float flux_dev(const RhsConsts& C, int v, const PtF& 
   }
 }
 
-template <int DIR>
-__device__ __forceinline__ float wave_speed_f(const RhsConsts& C, const PtF& s) {
+template <int DIR, class TC>
+__device__ __forceinline__ float wave_speed_f(const TC& C, const PtF& s) {
   const float arg = (float)C.g * s.h + s.p + (float)C.c2;
   return fabsf(DIR == 0 ? s.u : s.v) + sqrtf(fmaxf(arg, 0.0f));
 }
 
 // Hydrostatic part of the normal momentum flux, FP64: 0.5 g (h^2 - H^2) as
 // 0.5 g (h - H)(h + H), which is exact at rest and cancels no digits.
-__device__ __forceinline__ double hydro64(const RhsConsts& C, double h, double Hl) {
+template <class TC>
+__device__ __forceinline__ double hydro64(const TC& C, double h, double Hl) {
   return C.halfg * ((h - Hl) * (h + Hl));
 }
 
@@ -146,8 +148,8 @@ __device__ __forceinline__ double hydro64(const RhsConsts& C, double h, double H
 //   h[k]      full depth at the nodes (FP64), Hn[k] nodal still depth
 //   qf[k][4]  FP32 hu, hv, hw, hp at the nodes
 //   nh, nq    the neighbour node across each face (FP64 depth, FP32 discharges)
-template <int DIR, class EmitN, class Emit>
-__device__ __forceinline__ void line_mixed(const RhsConsts& C, const double (&h)[NP],
+template <int DIR, class TC, class TB, class EmitN, class Emit>
+__device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const double (&h)[NP],
                                            const double (&Hn)[NP], const float (&qf)[NP][4],
                                            double nhLo, const float* nqLo, double nhHi,
                                            const float* nqHi, double HfLo, double HfHi,
@@ -195,13 +197,13 @@ __device__ __forceinline__ void line_mixed(const RhsConsts& C, const double (&h)
   const double iJ64 = DIR == 0 ? C.iJx : C.iJy;
 #pragma unroll
   for (int m = 0; m < NP; ++m) {
-    const float gL = (float)C.gLp[m], gR = (float)C.gRp[m];
+    const float gL = (float)Tb.gLp[m], gR = (float)Tb.gRp[m];
     float se = jeLo * gL + jeHi * gR;
-    double sh = jHydLo * C.gLp[m] + jHydHi * C.gRp[m];
+    double sh = jHydLo * Tb.gLp[m] + jHydHi * Tb.gRp[m];
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      se = fmaf((float)C.D[m * NP + k], eta[k], se);
-      sh = fma(C.D[m * NP + k], hyd[k], sh);
+      se = fmaf((float)Tb.D[m * NP + k], eta[k], se);
+      sh = fma(Tb.D[m * NP + k], hyd[k], sh);
     }
     emit_node(m, se * iJ, sh * iJ64, s[m], eta[m]);
   }
@@ -212,19 +214,20 @@ __device__ __forceinline__ void line_mixed(const RhsConsts& C, const double (&h)
     for (int k = 0; k < NP; ++k) F[k] = flux_dev<DIR>(C, v, s[k]);
 #pragma unroll
     for (int m = 0; m < NP; ++m) {
-      float a = jLo[v] * (float)C.gLp[m];
-      a = fmaf(jHi[v], (float)C.gRp[m], a);
+      float a = jLo[v] * (float)Tb.gLp[m];
+      a = fmaf(jHi[v], (float)Tb.gRp[m], a);
 #pragma unroll
-      for (int k = 0; k < NP; ++k) a = fmaf((float)C.D[m * NP + k], F[k], a);
+      for (int k = 0; k < NP; ++k) a = fmaf((float)Tb.D[m * NP + k], F[k], a);
       emit(m, v, a * iJ, s[m]);
     }
   }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const StageArgsM A) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+// One tile (bx, by) of the mixed-precision right-hand side / stage kernel, error partial
+// slot blk. Shared by the single-instance kernel and the batched kernel.
+template <int MODE, class TC, class TB, class TA>
+__device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& A, int bx, int by,
+                                           long long blk, Smem& S) {
 
   int cur = 0;
   double atol = 0.0, rtol = 0.0;
@@ -246,11 +249,12 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
   I.k2 = A.K2;
   I.k3 = A.K3;
 
-  const int tid = threadIdx.x;
+  int tid;  // opaque: keeps per-thread descriptors out of the batched kernel's tile loop
+  asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
   const int warp = tid >> 5, lane = tid & 31;
   const int Nx = C.Nx, Ny = C.Ny;
   const long long Nd = C.Nd;
-  const int ex0 = blockIdx.x * TX, ey0 = blockIdx.y * TY;
+  const int ex0 = bx * TX, ey0 = by * TY;
   const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
   const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
   const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
@@ -449,10 +453,10 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
     const double HfHi = (iy + 1 < TYv) ? hf_y(S, i + TX, j) : hf_yt(S, ix, j);
     float hydv[NP];
     line_mixed<1>(
-        C, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
+        C, Tb, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
         [&](int b, float deta, double dhyd, const PtF& s, float) {
           const int loc = j + NP * b;
-          const double Hyl = depth_grad<1>(C, S.H[i], j, b);
+          const double Hyl = depth_grad<1>(C, Tb, S.H[i], j, b);
           // ncpY with h_y = D eta + H_y (sgn_flux2d.h:156-161)
           S.G[NV][i][loc] = mc2f * s.v * (deta + (float)Hyl);
           // y hydrostatic part of dU[HV]: -d_y hyd + g (h - H) H_y, cancelled in FP64
@@ -492,9 +496,9 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
     const double HfHi = (ix + 1 < TXv) ? hf_x(S, i + 1, j) : hf_xr(S, iy, j);
     float hydu[NP], Bx[NP], Hxf[NP];
     line_mixed<0>(
-        C, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
+        C, Tb, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
         [&](int a, float deta, double dhyd, const PtF& s, float) {
-          const double Hxl = depth_grad<0>(C, S.H[i], a, j);
+          const double Hxl = depth_grad<0>(C, Tb, S.H[i], a, j);
           Bx[a] = mc2f * s.u * (deta + (float)Hxl);  // ncpX
           hydu[a] = (float)(C.g * (h[a] - Hn[a]) * Hxl - dhyd);
           Hxf[a] = (float)Hxl;
@@ -508,11 +512,11 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
           } else if (v == 1) {
             res = hydu[a] + gammaf * s.p * Hxf[a] - (d + g);
           } else if (v == 2) {
-            res = gammaf * s.p * (float)depth_grad<1>(C, S.H[i], a, j) - (d + g);
+            res = gammaf * s.p * (float)depth_grad<1>(C, Tb, S.H[i], a, j) - (d + g);
           } else if (v == 3) {
             res = gammaf * s.p - (d + g);
           } else {
-            const float Hxl = Hxf[a], Hyl = (float)depth_grad<1>(C, S.H[i], a, j);
+            const float Hxl = Hxf[a], Hyl = (float)depth_grad<1>(C, Tb, S.H[i], a, j);
             const float S4 = (float)C.m2c2 * (s.w + s.u * Hxl + s.v * Hyl);
             res = S4 - (d + g) - Bx[a] - S.G[NV][i][loc];
           }
@@ -614,11 +618,61 @@ __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const Stag
         m = m < S.red[w][1] ? S.red[w][1] : m;
         n += S.red[w][2];
       }
-      const long long blk = (long long)blockIdx.y * gridDim.x + blockIdx.x;
       A.partials[3 * blk + 0] = s;
       A.partials[3 * blk + 1] = m;
       A.partials[3 * blk + 2] = n;
     }
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const StageArgsM A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  mixed_tile<MODE>(C, C, A, blockIdx.x, blockIdx.y,
+                   (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
+}
+
+// Batched form (8x4 tiles): the work list of BatchArgsM, per tile the instance's constants
+// and buffer pointers copied into shared memory and read through volatile views.
+// PERSIST: a fixed grid loops over the list; otherwise one CTA per tile.
+template <int MODE>
+__device__ __forceinline__ void mixed_batch_tile(const BatchArgsM& B, long long t, Smem& S,
+                                                 RhsConsts& Cs, StageArgsM& As) {
+  const int inst = B.tile_inst[t];
+  const long long lt = t - B.tile_start[inst];
+  __syncthreads();  // the previous tile is done with Cs / As
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(B.consts + inst);
+    unsigned* dst = reinterpret_cast<unsigned*>(&Cs);
+    for (int w = threadIdx.x; w < (int)(sizeof(RhsConsts) / 4); w += NTHR) dst[w] = src[w];
+    const unsigned* srca = reinterpret_cast<const unsigned*>(B.args + inst);
+    unsigned* dsta = reinterpret_cast<unsigned*>(&As);
+    for (int w = threadIdx.x; w < (int)(sizeof(StageArgsM) / 4); w += NTHR) dsta[w] = srca[w];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    As.kin_k2 = B.kin_k2;
+    As.coef = B.coef;
+    if (MODE == MODE_STAGE) As.out = B.kin_k2 ? As.K3 : As.K2;
+  }
+  __syncthreads();
+  const int ntx = (Cs.Nx + TX - 1) / TX;
+  mixed_tile<MODE>(static_cast<const volatile RhsConsts&>(Cs), B.tables,
+                   static_cast<const volatile StageArgsM&>(As), (int)(lt % ntx), (int)(lt / ntx),
+                   lt, S);
+}
+
+template <int MODE, bool PERSIST>
+__global__ void __launch_bounds__(NTHR, 3) k_mixed_batch(const BatchArgsM B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  __shared__ RhsConsts Cs;
+  __shared__ StageArgsM As;
+  if constexpr (PERSIST) {
+    for (long long t = blockIdx.x; t < B.ntiles; t += gridDim.x) mixed_batch_tile<MODE>(B, t, S, Cs, As);
+  } else {
+    if ((long long)blockIdx.x < B.ntiles) mixed_batch_tile<MODE>(B, blockIdx.x, S, Cs, As);
   }
 }
 

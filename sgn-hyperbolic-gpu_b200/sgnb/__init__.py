@@ -465,7 +465,8 @@ def _stats(st) -> AdaptiveRKStats:
 
 
 class SGNBatch:
-    """Many independent SGN2D instances advanced together (FP64_FAST).
+    """Many independent SGN2D instances advanced together (FP64_FAST, or MIXED with
+    ``precision=MIXED``).
 
     ``instances`` is a list of keyword dicts for SGN2DB200 (mesh size, domain, c, gamma,
     boundaries, bathymetry). Every RK stage is one persistent launch over the tiles of all
@@ -473,12 +474,12 @@ class SGNBatch:
     instance i with the single-instance methods (upload, download, rhs, mass, ...).
     """
 
-    def __init__(self, instances, device=0):
+    def __init__(self, instances, device=0, precision=FP64_FAST):
         self._b = None
         holders = []
         for kw in instances:
             kw = dict(kw)
-            kw.setdefault("precision", FP64_FAST)
+            kw.setdefault("precision", precision)
             kw["device"] = device
             args = [kw.pop(k, dflt) for k, dflt in (
                 ("P", 4), ("Nx", 8), ("Ny", 6), ("Lx", 10.0), ("Ly", 8.0), ("g", 9.81),

@@ -5,7 +5,8 @@ on the stream the work runs on, after warm-up, with the state resident in HBM.
 
 sweep    configuration 4: 256 instances (workloads.cfg4_instances) advanced K accepted
          steps each by the batched launches (after the autotuner), against the same
-         instances run one after another through the single-instance device loop.
+         instances run one after another through the single-instance device loop; FP64
+         (fast) or, with --precision mixed, the mixed-precision form on both sides.
 mixed    configuration 2 in FP64 (fast) and in the mixed-precision mode, K steps each,
          and the free-surface error of the mixed mode against FP64: every mode replays
          two step sequences from the same state (constant 0.4 x the CFL-0.5 step, and the
@@ -45,7 +46,8 @@ def run_sweep(args, clock_sampler, peak):
 
     inst = W.cfg4_instances()
     n = len(inst)
-    b = SGNBatch(inst)
+    mixed = args.precision == "mixed"
+    b = SGNBatch(inst, precision=MIXED if mixed else FP64_FAST)
     dofs = np.array([125.0 * k["Nx"] * k["Ny"] for k in inst])
     dt0 = np.zeros(n)
 
@@ -91,12 +93,12 @@ def run_sweep(args, clock_sampler, peak):
     seq_value = rhs_seq / t_seq
     shape, blocks = b.config
     best_ms = float(tune.min())
-    achieved = STAGE_LOOP_BYTES * dofs.sum() / (best_ms / 1e3) / 1e9
+    achieved = (MIXED_LOOP_BYTES if mixed else STAGE_LOOP_BYTES) * dofs.sum() / (best_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_batch / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 state, f32 deviations" if mixed else "f64", "data": "synthetic",
         "config": {"workload": "configuration 4: 256 instances (Nx U{64..512}, Ny U{32..256}, "
                                "alpha U[1.5,6], shoal crest U[0.3,0.9], Gaussian hump), "
                                "walls, per-instance adaptive BS3(2), K accepted steps each",
@@ -107,7 +109,7 @@ def run_sweep(args, clock_sampler, peak):
                    "l2": f"inputs larger than L2 ({8 * dofs.sum() / 1e9:.1f} GB per state)"},
         "sequential_single_instance": {"value": seq_value, "unit": UNIT, "time_s": t_seq},
         "speedup_vs_sequential": value / seq_value,
-        "autotune_ms_per_attempt": {"shapes": ["8x4", "16x2", "4x8"],
+        "autotune_ms_per_attempt": {"shapes": ["8x4", "16x2", "4x8 (-1: not used)"],
                                     "grids": ["per tile", "1/SM", "2/SM", "3/SM", "4/SM"],
                                     "ms": np.round(tune, 3).tolist()},
         "roofline": {"bound": "hbm", "kernel": "batched stage kernels, one attempt",

@@ -164,3 +164,31 @@ def test_sweep_generator_shapes():
         h = d.download()[: d.Nd]
         eta = 0.05 * np.exp(-((x - 6.0) ** 2 + (y - 5.0) ** 2) / 0.5)
         assert np.abs(h - (H + eta)).max() < 1e-14
+
+
+def test_mixed_batch_matches_single_runs():
+    """The mixed-precision batch (8x4 tiles) against mixed single-instance runs."""
+    cases = small_batch(seed=13)
+    dt0 = dt0_of(cases)
+    ref = []
+    for (kw, U), d0 in zip(cases, dt0):
+        with sgnb.SGN2DB200(precision=sgnb.MIXED, **kw) as d:
+            d.upload(U)
+            st = d.integrate_steps(0.0, d0, 10)
+            ref.append((d.download(), st))
+    b = sgnb.SGNBatch([kw for kw, _ in cases], precision=sgnb.MIXED)
+    with b:
+        for i, (_, U) in enumerate(cases):
+            b[i].upload(U)
+        ms = b.autotune(dt0, reps=2)
+        assert np.all(ms[0] > 0) and np.all(ms[1:] == -1.0) and b.config[0] == 0
+        with pytest.raises(sgnb.SgnbError):
+            b.config = (1, 0)
+        for grid in (0, 2 * 148):
+            for i, (_, U) in enumerate(cases):
+                b[i].upload(U)
+            b.config = (0, grid)
+            stats = b.integrate_steps(dt0, 10)
+            for i, (U1, st1) in enumerate(ref):
+                assert rel_per_field(b[i].download(), U1) < 1e-6, f"instance {i}"
+                assert stats[i].accepted == 10 and stats[i].rejected == st1.rejected
