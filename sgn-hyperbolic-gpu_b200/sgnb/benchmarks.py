@@ -92,7 +92,7 @@ def run_sweep(args, clock_sampler, peak):
         rhs_seq += dofs[i] * si.rhsEvals
     seq_value = rhs_seq / t_seq
     shape, blocks = b.config
-    best_ms = float(tune.min())
+    best_ms = float(tune[tune > 0].min())  # -1 marks shapes a mixed batch does not use
     achieved = (MIXED_LOOP_BYTES if mixed else STAGE_LOOP_BYTES) * dofs.sum() / (best_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
