@@ -9,8 +9,9 @@
 //   j = F* - F(own trace), dF_m = (sum_k D[m,k] F_k + jLo gL'[m] + jHi gR'[m]) / J
 //   dh_m likewise with the central common depth            (sgn2d.cpp:265-275)
 //   R -= dF; R[hp] -= -c^2 u_n dh  (non-conservative term, sgn_flux2d.h:150-161)
-// plus the pointwise sources (sgn_flux2d.h:122-134). Given a cotangent Rb of R, the line
-// kernel reverses one line (one thread per element line and direction) and writes:
+// plus the pointwise sources (sgn_flux2d.h:122-142, Manning friction included). Given a
+// cotangent Rb of R, the line kernel reverses one line (one thread per element line and
+// direction) and writes:
 //   * the cotangent of the line's own nodes, per direction (each node lies on exactly one
 //     x line and one y line of its element, so these are plain stores);
 //   * the cotangent of the neighbour's trace node across each face (a per-face buffer the
@@ -96,18 +97,6 @@ __device__ __forceinline__ void wave_speed_back(const RhsConsts& C, const double
   double q[4] = {0.0, 0.0, 0.0, ab};
   q[DIR] = unb;
   prim_back(U, q[0], q[1], q[2], q[3], Ub);
-}
-
-template <int DIR>
-__device__ __forceinline__ void flux_fwd(const RhsConsts& C, const double* U, double H, double* F) {
-  constexpr int nd = 1 + DIR, td = 2 - DIR;
-  const double ih = 1.0 / U[0];
-  const double hn = U[nd];
-  F[0] = hn;
-  F[nd] = hn * (hn * ih) + C.halfg * (U[0] * U[0] - H * H) + U[4];
-  F[td] = hn * (U[td] * ih);
-  F[3] = hn * (U[3] * ih);
-  F[4] = hn * (U[4] * ih + C.c2);
 }
 
 // One line: reverse of its contribution to R (see the file comment).
@@ -305,8 +294,22 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
       Hb[m] -= C.g * sHr;
       A.Hxb[g] = bath * r1 + C.m2c2 * u * r4;
       A.Hyb[g] = bath * r2 + C.m2c2 * v * r4;
-      prim_back(U, C.m2c2 * Hx * r4, C.m2c2 * Hy * r4, C.m2c2 * r4,
-                C.gamma * sHr + C.gamma * r3, Ub[m]);
+      double ub = C.m2c2 * Hx * r4, vb = C.m2c2 * Hy * r4;
+      if (C.manning) {
+        // friction (-cf u, -cf v), cf = n^2 g |vel| h^(-1/3)
+        const double vm = sqrt(u * u + v * v);
+        const double kc = C.n2g / cbrt(U[0]);
+        const double cf = kc * vm;
+        const double ruv = r1 * u + r2 * v;
+        ub -= r1 * cf;
+        vb -= r2 * cf;
+        if (vm > 0.0) {
+          ub -= kc * ruv * u / vm;
+          vb -= kc * ruv * v / vm;
+        }
+        Ub[m][0] += ruv * cf / (3.0 * U[0]);  // d/dh of h^(-1/3)
+      }
+      prim_back(U, ub, vb, C.m2c2 * r4, C.gamma * sHr + C.gamma * r3, Ub[m]);
     }
   }
 

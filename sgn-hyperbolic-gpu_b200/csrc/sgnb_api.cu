@@ -98,8 +98,7 @@ int check_desc(const sgnb_desc* d) {
   if (d->Nx < 2 || d->Ny < 2) return fail(nullptr, SGNB_ERR_INVALID, "SGN2D: Nx,Ny >= 2");
   if (d->P != 4) return fail(nullptr, SGNB_ERR_UNSUPPORTED, "only P = 4 is built");
   if (!(d->Lx > 0) || !(d->Ly > 0)) return fail(nullptr, SGNB_ERR_INVALID, "Lx, Ly must be > 0");
-  if (d->nManning != 0.0)
-    return fail(nullptr, SGNB_ERR_UNSUPPORTED, "Manning friction is not built");
+  if (!(d->nManning >= 0.0)) return fail(nullptr, SGNB_ERR_INVALID, "nManning must be >= 0");
   if (d->bc_x < 0 || d->bc_x > 1 || d->bc_y < 0 || d->bc_y > 1)
     return fail(nullptr, SGNB_ERR_INVALID, "bc must be SGNB_BC_PERIODIC or SGNB_BC_WALL");
   if (d->precision != SGNB_FP64_EXACT && d->precision != SGNB_FP64_FAST &&
@@ -159,6 +158,8 @@ void fill_consts(sgnb_ctx* c) {
   C.c2 = d.c * d.c;
   C.mc2 = -d.c * d.c;
   C.m2c2 = -2.0 * C.c2;
+  C.n2g = (d.nManning * d.nManning) * d.g;  // n2 * g as sgn_flux2d.h:137-139 multiplies
+  C.manning = d.nManning != 0.0;
   C.Jx = 0.5 * c->mesh.hx;  // mesh2d.h:49-50
   C.Jy = 0.5 * c->mesh.hy;
   C.iJx = 1.0 / C.Jx;

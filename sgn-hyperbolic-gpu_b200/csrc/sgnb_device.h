@@ -18,6 +18,9 @@ struct RhsConsts {
   double c2;           // c * c
   double mc2;          // (-c) * c, the ncp coefficient
   double m2c2;         // -2.0 * c2, the relaxation-source coefficient
+  double n2g;          // nManning^2 * g: Manning friction (sgn_flux2d.h:135-142)
+  int manning;         // friction on (nManning != 0)
+  int pad_;
   double Jx, Jy;       // affine Jacobians hx/2, hy/2
   double iJx, iJy;     // 1/Jx, 1/Jy (fast mode)
   double D[25];        // GLL differentiation matrix, row-major

@@ -698,8 +698,15 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             res = EXACT ? (-d - g) + S3 : S3 - (d + g);
           } else if (v == 1 || v == 2) {
             const double bath = C.g * (Un[a][0] - Hn[a]) + C.gamma * q.p;
-            const double Sv = bath * (v == 1 ? depth_grad<EXACT, 0>(C, Tb, S.H[i], a, j)
-                                             : depth_grad<EXACT, 1>(C, Tb, S.H[i], a, j));
+            double Sv = bath * (v == 1 ? depth_grad<EXACT, 0>(C, Tb, S.H[i], a, j)
+                                       : depth_grad<EXACT, 1>(C, Tb, S.H[i], a, j));
+            if (C.manning) {
+              // Manning friction along the velocity, n^2 g |vel| vel / h^(1/3)
+              // (sgn_flux2d.h:135-142)
+              const double vmag = sqrt(q.u * q.u + q.v * q.v);
+              const double cf = C.n2g * vmag / cbrt(Un[a][0]);
+              Sv = Sv - cf * (v == 1 ? q.u : q.v);
+            }
             res = EXACT ? (-d - g) + Sv : Sv - (d + g);
           } else {
             const double Hxl = depth_grad<EXACT, 0>(C, Tb, S.H[i], a, j);

@@ -509,10 +509,14 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           float res;
           if (v == 0) {
             res = -(d + g);
-          } else if (v == 1) {
-            res = hydu[a] + gammaf * s.p * Hxf[a] - (d + g);
-          } else if (v == 2) {
-            res = gammaf * s.p * (float)depth_grad<1>(C, Tb, S.H[i], a, j) - (d + g);
+          } else if (v == 1 || v == 2) {
+            // Manning friction n^2 g |vel| vel / h^(1/3), a deviation term (FP32)
+            float fr = 0.0f;
+            if (C.manning)
+              fr = (float)C.n2g * sqrtf(s.u * s.u + s.v * s.v) / cbrtf(s.h) *
+                   (v == 1 ? s.u : s.v);
+            res = v == 1 ? hydu[a] + gammaf * s.p * Hxf[a] - fr - (d + g)
+                         : gammaf * s.p * (float)depth_grad<1>(C, Tb, S.H[i], a, j) - fr - (d + g);
           } else if (v == 3) {
             res = gammaf * s.p - (d + g);
           } else {

@@ -49,9 +49,11 @@ def oracle_rhs(o, U, S):
     return o.rhs(U)
 
 
-@pytest.mark.parametrize("bc", [sgnb.BC_PERIODIC, sgnb.BC_WALL])
-def test_rhs_vjp_against_oracle_differences(bc):
+@pytest.mark.parametrize("bc,manning", [(sgnb.BC_PERIODIC, 0.0), (sgnb.BC_WALL, 0.0),
+                                        (sgnb.BC_WALL, 0.03)])
+def test_rhs_vjp_against_oracle_differences(bc, manning):
     kw, U = rhs_case(bc)
+    kw = dict(kw, nManning=manning)
     rng = np.random.default_rng(10 + bc)
     o = O.Oracle(**kw)
     S0 = o.bathymetry()

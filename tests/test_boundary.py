@@ -72,7 +72,7 @@ def test_host_bathymetry_bitwise(kind, par, bc):
 @pytest.mark.parametrize("kw,code", [
     (dict(P=3), 2),             # only P = 4 is built
     (dict(Nx=1), 1),            # SGN2D: Nx, Ny >= 2 (src/solver/sgn2d.cpp:36)
-    (dict(nManning=0.02), 2),   # Manning friction not built
+    (dict(nManning=-0.02), 1),  # Manning coefficient must be >= 0
     (dict(bc_x=7), 1),
     (dict(precision=9), 2),
     (dict(bathy_kind=42), 1),

@@ -42,6 +42,17 @@ def test_rhs_bitwise_vs_reference(need_reference, bcx, bcy):
         assert bits_equal(ba["HfaceYEnd"], bb["HfaceYEnd"])
 
 
+@pytest.mark.parametrize("bc", [0, 1])
+def test_rhs_manning_bitwise_vs_reference(need_reference, bc):
+    """Manning friction branch (sgn_flux2d.h:135-142), n = 0.03."""
+    kw, U = bump_case(bc)
+    kw = dict(kw, nManning=0.03)
+    a, b = oracle_for(kw), oracle_for(kw, reference=True)
+    Ra = a.rhs(U)
+    assert bits_equal(Ra, b.rhs(U))
+    assert not bits_equal(Ra, oracle_for(dict(kw, nManning=0.0)).rhs(U))
+
+
 @pytest.mark.parametrize("Nx,Ny", [(2, 2), (3, 5), (10, 6)])
 def test_rhs_bitwise_vs_reference_sizes(need_reference, Nx, Ny):
     kw, U = bump_case(Nx=Nx, Ny=Ny)

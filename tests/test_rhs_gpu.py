@@ -40,6 +40,23 @@ def test_bump_exact_bitwise_and_fast(bcx, bcy):
         assert rel_per_field(d.rhs(U), R) < FAST_TOL
 
 
+@pytest.mark.parametrize("bc", [0, 1])
+def test_manning_friction(bc):
+    """Manning friction (n = 0.03): the exact mode matches the oracle to the last-bit
+    rounding of cbrt (the device's and the host's cube roots may round differently), the
+    fast mode within 1e-13, the mixed mode within its FP32 tolerance."""
+    kw, U = bump_case(bc)
+    kw = dict(kw, nManning=0.03)
+    R = O.Oracle(**kw).rhs(U)
+    assert not bits_equal(R, O.Oracle(**dict(kw, nManning=0.0)).rhs(U))
+    with device(kw, sgnb.FP64_EXACT) as d:
+        assert rel_per_field(d.rhs(U), R) < 1e-15
+    with device(kw, sgnb.FP64_FAST) as d:
+        assert rel_per_field(d.rhs(U), R) < FAST_TOL
+    with device(kw, sgnb.MIXED) as d:
+        assert rel_per_field(d.rhs(U), R) < 2e-5
+
+
 def test_golden_fixture_bitwise(golden):
     """The reference's own rhs of its GPU-parity case, from the committed fixture."""
     for tag, bc in (("bump", 0), ("wall", 1)):
