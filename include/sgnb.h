@@ -198,6 +198,18 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
                           double* HfaceX, double* HfaceY, double* HfaceXEnd,
                           double* HfaceYEnd);
 
+/* Device-side sampling for the reference's applications, which download the whole state
+ * at every sample time and scan it on the host (apps/shoal_focus_mpi.cu:195-205,
+ * apps/tsunami_margin_mpi.cu:184-198). sgnb_eta_max: the largest eta = h - H of the
+ * current state over the nodes inside [x0, x1] x [y0, y1] (bounds inclusive; +-HUGE_VAL for
+ * none) and the node holding it (smallest index on ties; -1 and -HUGE_VAL when the
+ * window holds no node). sgnb_sample_eta: eta at n nodes (gauges). sgnb_nearest_node: the
+ * node closest to (x, y) (smallest index on ties), as the applications place gauges. */
+int sgnb_eta_max(sgnb_ctx* ctx, double x0, double x1, double y0, double y1, double* eta_max,
+                 long long* node);
+int sgnb_sample_eta(sgnb_ctx* ctx, const long long* nodes, int n, double* eta);
+int sgnb_nearest_node(const sgnb_ctx* ctx, double x, double y, long long* node);
+
 /* Batched sweep (no reference counterpart; the reference runs one instance per
  * SGN2DCuda): n independent instances (their own mesh size, parameters, bathymetry and
  * state) advanced together, one launch per RK stage over all instances' tiles, each

@@ -418,6 +418,7 @@ int sgnb_destroy(sgnb_ctx* c) {
   cudaFree(c->K2);  // K3 lives in the same block
   cudaFree(c->partials); cudaFree(c->diag); cudaFree(c->dctrl); cudaFree(c->dtList);
   cudaFree(c->alog);
+  cudaFree(c->gauge);
   if (c->hctrl) cudaFreeHost(c->hctrl);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -829,6 +830,74 @@ int batch_run(sgnb_batch* b) {
 }  // namespace
 
 extern "C" {
+
+int sgnb_eta_max(sgnb_ctx* c, double x0, double x1, double y0, double y1, double* eta_max,
+                 long long* node) {
+  if (!c || !eta_max || !node) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  const int nblk = c->ndiag / 2;
+  SGNB_CU(c, dev::launch_eta_max(c->C, c->U[c->cur], x0, x1, y0, y1, c->mesh.hx, c->mesh.hy,
+                                 c->tab.nodes, c->diag, nblk, c->stream));
+  std::vector<double> part(2 * (size_t)nblk);
+  SGNB_CU(c, cudaMemcpyAsync(part.data(), c->diag, part.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  double best = -HUGE_VAL;
+  long long bi = -1;
+  for (int b = 0; b < nblk; ++b) {
+    const long long i = (long long)part[2 * b + 1];
+    if (i < 0) continue;
+    if (bi < 0 || part[2 * b] > best || (part[2 * b] == best && i < bi)) {
+      best = part[2 * b];
+      bi = i;
+    }
+  }
+  *eta_max = best;
+  *node = bi;
+  return SGNB_OK;
+}
+
+int sgnb_sample_eta(sgnb_ctx* c, const long long* nodes, int n, double* eta) {
+  if (!c || n < 0 || (n > 0 && (!nodes || !eta))) return fail(c, SGNB_ERR_INVALID, "bad arguments");
+  if (n == 0) return SGNB_OK;
+  for (int k = 0; k < n; ++k)
+    if (nodes[k] < 0 || nodes[k] >= c->Nd) return fail(c, SGNB_ERR_INVALID, "node out of range");
+  if (int rc = set_device(c)) return rc;
+  if (n > c->gaugeCap) {
+    cudaFree(c->gauge);
+    c->gauge = nullptr;
+    c->gaugeCap = 0;
+    SGNB_CU(c, cudaMalloc(&c->gauge, 2 * (size_t)n * sizeof(double)));
+    c->gaugeCap = n;
+  }
+  long long* dn = reinterpret_cast<long long*>(c->gauge);
+  double* dv = c->gauge + c->gaugeCap;
+  SGNB_CU(c, cudaMemcpyAsync(dn, nodes, n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  SGNB_CU(c, dev::launch_sample_eta(c->U[c->cur], c->C.Hnod, dn, n, dv, c->stream));
+  SGNB_CU(c, cudaMemcpyAsync(eta, dv, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SGNB_CU(c, cudaStreamSynchronize(c->stream));
+  return SGNB_OK;
+}
+
+int sgnb_nearest_node(const sgnb_ctx* c, double x, double y, long long* node) {
+  if (!c || !node) return SGNB_ERR_INVALID;
+  // the node coordinates of node_coords, scanned per element in index order
+  const int Nx = c->desc.Nx, Ny = c->desc.Ny;
+  double best = HUGE_VAL;
+  long long bi = -1;
+  for (long long e = 0; e < (long long)Nx * Ny; ++e) {
+    const int ex = (int)(e % Nx), ey = (int)(e / Nx);
+    for (int b = 0; b < 5; ++b)
+      for (int a = 0; a < 5; ++a) {
+        const double xn = ex * c->mesh.hx + 0.5 * c->mesh.hx * (c->tab.nodes[a] + 1.0);
+        const double yn = ey * c->mesh.hy + 0.5 * c->mesh.hy * (c->tab.nodes[b] + 1.0);
+        const double d2 = (xn - x) * (xn - x) + (yn - y) * (yn - y);
+        if (d2 < best) { best = d2; bi = e * 25 + a + 5 * b; }
+      }
+  }
+  *node = bi;
+  return SGNB_OK;
+}
 
 int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
   if (!out || !descs || n < 1) return bfail(nullptr, SGNB_ERR_INVALID, "descs, n >= 1, out");

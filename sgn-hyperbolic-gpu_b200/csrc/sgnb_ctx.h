@@ -42,6 +42,8 @@ struct sgnb_ctx {
   cudaEvent_t evRead = nullptr;
   long long launches = 0;  // kernels launched by the last integration
   long long pendingMaxAccepted = 0;  // set by sgnb_integrate_steps
+  double* gauge = nullptr;  // gauge sampling: nodes then values, grown on demand
+  int gaugeCap = 0;
   int cur = 0;
   std::string err;
 };

@@ -193,6 +193,13 @@ size_t fused_smem_bytes();
 // partials, accept/reject, PI step-size update and the next attempt's dt.
 cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk,
                               long long n, cudaStream_t s);
+// Largest eta = h - H inside a window, with its node: (value, index) per block.
+cudaError_t launch_eta_max(const RhsConsts& C, const double* U, double x0, double x1, double y0,
+                           double y1, double hx, double hy, const double* xi, double* out,
+                           int nblk, cudaStream_t s);
+// eta at the given nodes (gauges).
+cudaError_t launch_sample_eta(const double* U, const double* Hnod, const long long* nodes, int n,
+                              double* out, cudaStream_t s);
 // Reductions over the uploaded state (diagnostics).
 cudaError_t launch_reduce_diag(int what, const RhsConsts& C, const double* U,
                                const double* qw, double* out_partials, int nblk,

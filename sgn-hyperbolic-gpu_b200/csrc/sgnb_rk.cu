@@ -179,5 +179,75 @@ cudaError_t launch_reduce_diag(int what, const RhsConsts& C, const double* U, co
   return cudaGetLastError();
 }
 
+// Largest eta = h - H over the nodes inside the window [x0, x1] x [y0, y1] and the node that
+// holds it (smallest index on ties), per block; the node coordinates are formed as the
+// set-up forms them (node_coords, sgnb_setup.cpp), so the window test agrees with the host.
+struct EtaWin {
+  double x0, x1, y0, y1, hx, hy;
+  double xi[5];
+};
+
+__global__ void __launch_bounds__(256) k_eta_max(const RhsConsts C, const double* U,
+                                                 const EtaWin W, double* out) {
+  __shared__ double sv[256];
+  __shared__ long long si[256];
+  const long long Nd = C.Nd;
+  double best = -HUGE_VAL;
+  long long bi = -1;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < Nd;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long e = i / 25;
+    const int loc = (int)(i - e * 25);
+    const int ex = (int)(e % C.Nx), ey = (int)(e / C.Nx);
+    const double x = ex * W.hx + 0.5 * W.hx * (W.xi[loc % 5] + 1.0);
+    const double y = ey * W.hy + 0.5 * W.hy * (W.xi[loc / 5] + 1.0);
+    if (x < W.x0 || x > W.x1 || y < W.y0 || y > W.y1) continue;
+    const double eta = U[i] - C.Hnod[i];
+    if (eta > best) { best = eta; bi = i; }  // grid-stride order: first index wins ties
+  }
+  sv[threadIdx.x] = best;
+  si[threadIdx.x] = bi;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if (threadIdx.x < off) {
+      const double ov = sv[threadIdx.x + off];
+      const long long oi = si[threadIdx.x + off];
+      if (oi >= 0 && (si[threadIdx.x] < 0 || ov > sv[threadIdx.x] ||
+                      (ov == sv[threadIdx.x] && oi < si[threadIdx.x]))) {
+        sv[threadIdx.x] = ov;
+        si[threadIdx.x] = oi;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = sv[0];
+    out[2 * blockIdx.x + 1] = (double)si[0];  // exact below 2^53
+  }
+}
+
+cudaError_t launch_eta_max(const RhsConsts& C, const double* U, double x0, double x1, double y0,
+                           double y1, double hx, double hy, const double* xi, double* out,
+                           int nblk, cudaStream_t s) {
+  EtaWin W;
+  W.x0 = x0; W.x1 = x1; W.y0 = y0; W.y1 = y1; W.hx = hx; W.hy = hy;
+  for (int k = 0; k < 5; ++k) W.xi[k] = xi[k];
+  k_eta_max<<<nblk, 256, 0, s>>>(C, U, W, out);
+  return cudaGetLastError();
+}
+
+// eta at the given nodes
+__global__ void k_sample_eta(const double* U, const double* Hnod, const long long* nodes, int n,
+                             double* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = U[nodes[k]] - Hnod[nodes[k]];
+}
+
+cudaError_t launch_sample_eta(const double* U, const double* Hnod, const long long* nodes, int n,
+                              double* out, cudaStream_t s) {
+  k_sample_eta<<<(n + 127) / 128, 128, 0, s>>>(U, Hnod, nodes, n, out);
+  return cudaGetLastError();
+}
+
 }  // namespace dev
 }  // namespace sgnb

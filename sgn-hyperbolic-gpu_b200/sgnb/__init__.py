@@ -140,6 +140,11 @@ SIGNATURES = {
                                         C.POINTER(C.c_void_p)]),
     "sgnb_fr_tables": (C.c_int, [C.c_int] + [_dp] * 7),
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
+    "sgnb_eta_max": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
+                               _dp, C.POINTER(C.c_longlong)]),
+    "sgnb_sample_eta": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int, _dp]),
+    "sgnb_nearest_node": (C.c_int, [C.c_void_p, C.c_double, C.c_double,
+                                    C.POINTER(C.c_longlong)]),
     "sgnb_batch_create": (C.c_int, [C.POINTER(_Desc), C.c_int, C.POINTER(C.c_void_p)]),
     "sgnb_batch_destroy": (C.c_int, [C.c_void_p]),
     "sgnb_batch_size": (C.c_int, [C.c_void_p]),
@@ -457,6 +462,29 @@ class SGN2DB200:
 
     def energy(self):
         return self._scalar(lib().sgnb_energy)
+
+    def eta_max(self, window=None):
+        """Largest eta = h - H of the current state inside window (x0, x1, y0, y1), the
+        whole domain by default, and its node index (-1 when the window holds no node)."""
+        inf = float("inf")
+        x0, x1, y0, y1 = window if window is not None else (-inf, inf, -inf, inf)
+        v = C.c_double()
+        n = C.c_longlong()
+        _check(lib().sgnb_eta_max(self._h, x0, x1, y0, y1, C.byref(v), C.byref(n)), self._h)
+        return v.value, n.value
+
+    def sample_eta(self, nodes):
+        """eta at the given node indices (gauges)."""
+        nd = np.ascontiguousarray(nodes, dtype=np.int64)
+        out = np.zeros(nd.size)
+        _check(lib().sgnb_sample_eta(self._h, nd.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                     int(nd.size), _ptr(out)), self._h)
+        return out
+
+    def nearest_node(self, x, y):
+        n = C.c_longlong()
+        _check(lib().sgnb_nearest_node(self._h, float(x), float(y), C.byref(n)), self._h)
+        return n.value
 
 
 def _stats(st) -> AdaptiveRKStats:
