@@ -209,6 +209,13 @@ int sgnb_eta_max(sgnb_ctx* ctx, double x0, double x1, double y0, double y1, doub
                  long long* node);
 int sgnb_sample_eta(sgnb_ctx* ctx, const long long* nodes, int n, double* eta);
 int sgnb_nearest_node(const sgnb_ctx* ctx, double x, double y, long long* node);
+/* Element means of eta = h - H, u, v, p and H of the current state (out: 5 * Nx * Ny,
+ * field-major, element ex + Nx ey), formed on the device as the reference's VTK writer
+ * forms them (src/io/vtk2d.h:38-44), and that writer's legacy-VTK frame
+ * (STRUCTURED_POINTS, ASCII, src/io/vtk2d.h:30-83) from them: only 5 Nx Ny values cross
+ * to the host instead of the state. */
+int sgnb_element_means(sgnb_ctx* ctx, double* out);
+int sgnb_write_vtk(sgnb_ctx* ctx, const char* path);
 
 /* Batched sweep (no reference counterpart; the reference runs one instance per
  * SGN2DCuda): n independent instances (their own mesh size, parameters, bathymetry and

@@ -74,6 +74,9 @@ def _load(path: str) -> C.CDLL:
     lib.or_ndof.argtypes = [C.c_void_p]
     lib.or_tables.argtypes = [C.c_void_p] + [_dp] * 7
     lib.or_bathymetry.argtypes = [C.c_void_p] + [_dp] * 7
+    if hasattr(lib, "or_write_vtk"):
+        lib.or_write_vtk.argtypes = [C.c_void_p, _dp, C.c_char_p]
+        lib.or_write_vtk.restype = C.c_int
     if hasattr(lib, "or_set_bathymetry"):
         lib.or_set_bathymetry.argtypes = [C.c_void_p] + [_dp] * 7
     lib.or_node_coords.argtypes = [C.c_void_p, _dp, _dp]
@@ -142,6 +145,14 @@ class Oracle:
         self.lib.or_bathymetry(self.h, *(_ptr(out[k]) for k in (
             "Hnod", "Hx", "Hy", "HfaceX", "HfaceY", "HfaceXEnd", "HfaceYEnd")))
         return out
+
+    def write_vtk(self, U, path):
+        """The reference's VTK frame writer (compiled reference only, periodic domains)."""
+        if not hasattr(self.lib, "or_write_vtk"):
+            raise NotImplementedError("write_vtk needs the compiled reference (reference=True)")
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if self.lib.or_write_vtk(self.h, _ptr(U), os.fsencode(path)) != 0:
+            raise ValueError("the reference writer runs on periodic domains only")
 
     def set_bathymetry(self, arrays):
         """Replaces the depth statics (keys as returned by bathymetry(); missing keys keep

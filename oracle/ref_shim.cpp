@@ -16,6 +16,7 @@
 
 #include "solver/rk.h"
 #include "solver/sgn2d.h"
+#include "io/vtk2d.h"
 
 #include <cstring>
 #include <memory>
@@ -115,6 +116,16 @@ or_ctx* or_create(int P, int Nx, int Ny, double Lx, double Ly, double g, double 
 }
 
 void or_destroy(or_ctx* s) { delete s; }
+
+/* [reference only] the reference's VTK frame writer (src/io/vtk2d.h) on a periodic
+ * domain; returns 0, or -1 when the domain has walls (mirror doubling would write the
+ * doubled domain). */
+int or_write_vtk(const or_ctx* s, const double* U, const char* path) {
+  if (s->bcx || s->bcy) return -1;
+  sgn::State Us(U, U + (size_t)sgn2d::NVAR * s->sys->nDof());
+  sgn::writeVtk2D(*s->sys, Us, path);
+  return 0;
+}
 
 long or_ndof(const or_ctx* s) { return s->ndof(); }
 

@@ -879,6 +879,46 @@ int sgnb_sample_eta(sgnb_ctx* c, const long long* nodes, int n, double* eta) {
   return SGNB_OK;
 }
 
+int sgnb_element_means(sgnb_ctx* c, double* out) {
+  if (!c || !out) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  if (int rc = set_device(c)) return rc;
+  const size_t n = 5 * (size_t)c->desc.Nx * c->desc.Ny;
+  double* d = nullptr;
+  SGNB_CU(c, cudaMalloc(&d, n * sizeof(double)));
+  cudaError_t e = dev::launch_elem_means(c->C, c->U[c->cur], c->tab.qw, d, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(c, e, "element means");
+  return SGNB_OK;
+}
+
+int sgnb_write_vtk(sgnb_ctx* c, const char* path) {
+  if (!c || !path) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  const int Nx = c->desc.Nx, Ny = c->desc.Ny;
+  const size_t ne = (size_t)Nx * Ny;
+  std::vector<double> m(5 * ne);
+  if (int rc = sgnb_element_means(c, m.data())) return rc;
+  std::FILE* fp = std::fopen(path, "w");
+  if (!fp) return fail(c, SGNB_ERR_INVALID, std::string("cannot open ") + path);
+  // legacy VTK, one point per element centre (the format of src/io/vtk2d.h:46-82)
+  std::fprintf(fp, "# vtk DataFile Version 3.0\nSGN2D element means\nASCII\n");
+  std::fprintf(fp, "DATASET STRUCTURED_POINTS\nDIMENSIONS %d %d 1\n", Nx, Ny);
+  std::fprintf(fp, "ORIGIN %.6f %.6f 0\nSPACING %.6f %.6f 1\n", 0.5 * c->mesh.hx,
+               0.5 * c->mesh.hy, c->mesh.hx, c->mesh.hy);
+  std::fprintf(fp, "POINT_DATA %d\n", Nx * Ny);
+  static const char* names[5] = {"eta", "u", "v", "p", "H"};
+  for (int f = 0; f < 5; ++f) {
+    std::fprintf(fp, "SCALARS %s float 1\nLOOKUP_TABLE default\n", names[f]);
+    for (int ey = 0; ey < Ny; ++ey) {
+      for (int ex = 0; ex < Nx; ++ex) std::fprintf(fp, "%.5e ", m[f * ne + ex + (size_t)Nx * ey]);
+      std::fprintf(fp, "\n");
+    }
+  }
+  const bool ok = std::fclose(fp) == 0;
+  return ok ? SGNB_OK : fail(c, SGNB_ERR_INVALID, std::string("write failed: ") + path);
+}
+
 int sgnb_nearest_node(const sgnb_ctx* c, double x, double y, long long* node) {
   if (!c || !node) return SGNB_ERR_INVALID;
   // the node coordinates of node_coords, scanned per element in index order

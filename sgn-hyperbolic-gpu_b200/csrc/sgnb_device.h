@@ -197,6 +197,9 @@ cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk,
 cudaError_t launch_eta_max(const RhsConsts& C, const double* U, double x0, double x1, double y0,
                            double y1, double hx, double hy, const double* xi, double* out,
                            int nblk, cudaStream_t s);
+// Element means of eta, u, v, p, H (out[f * ne + e]), as the reference's VTK writer forms them.
+cudaError_t launch_elem_means(const RhsConsts& C, const double* U, const double* qw, double* out,
+                              cudaStream_t s);
 // eta at the given nodes (gauges).
 cudaError_t launch_sample_eta(const double* U, const double* Hnod, const long long* nodes, int n,
                               double* out, cudaStream_t s);

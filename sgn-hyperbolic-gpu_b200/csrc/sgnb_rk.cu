@@ -236,6 +236,42 @@ cudaError_t launch_eta_max(const RhsConsts& C, const double* U, double x0, doubl
   return cudaGetLastError();
 }
 
+// Element means (GLL quadrature average: weights sum to 2 per direction, hence 0.25) of
+// eta = h - H, u, v, p and H, out[f * ne + e], in the order and rounding of the
+// reference's VTK writer (src/io/vtk2d.h:38-44, 69-81): s += qw[a] qw[b] f, then 0.25 s.
+__global__ void k_elem_means(const RhsConsts C, const double* U, const QW q, double* out) {
+  const long long ne = (long long)C.Nx * C.Ny;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const long long Nd = C.Nd;
+  for (int f = 0; f < 5; ++f) {
+    double s = 0.0;
+    for (int b = 0; b < 5; ++b)
+      for (int a = 0; a < 5; ++a) {
+        const long long i = e * 25 + a + 5 * b;
+        double val;
+        switch (f) {
+          case 0: val = U[i] - C.Hnod[i]; break;
+          case 1: val = U[Nd + i] / U[i]; break;
+          case 2: val = U[2 * Nd + i] / U[i]; break;
+          case 3: val = U[4 * Nd + i] / U[i]; break;
+          default: val = C.Hnod[i]; break;
+        }
+        s += q.w[a] * q.w[b] * val;
+      }
+    out[f * ne + e] = 0.25 * s;
+  }
+}
+
+cudaError_t launch_elem_means(const RhsConsts& C, const double* U, const double* qw, double* out,
+                              cudaStream_t s) {
+  QW q;
+  for (int k = 0; k < 5; ++k) q.w[k] = qw[k];
+  const long long ne = (long long)C.Nx * C.Ny;
+  k_elem_means<<<(unsigned)((ne + 127) / 128), 128, 0, s>>>(C, U, q, out);
+  return cudaGetLastError();
+}
+
 // eta at the given nodes
 __global__ void k_sample_eta(const double* U, const double* Hnod, const long long* nodes, int n,
                              double* out) {

@@ -145,6 +145,8 @@ SIGNATURES = {
     "sgnb_sample_eta": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int, _dp]),
     "sgnb_nearest_node": (C.c_int, [C.c_void_p, C.c_double, C.c_double,
                                     C.POINTER(C.c_longlong)]),
+    "sgnb_element_means": (C.c_int, [C.c_void_p, _dp]),
+    "sgnb_write_vtk": (C.c_int, [C.c_void_p, C.c_char_p]),
     "sgnb_batch_create": (C.c_int, [C.POINTER(_Desc), C.c_int, C.POINTER(C.c_void_p)]),
     "sgnb_batch_destroy": (C.c_int, [C.c_void_p]),
     "sgnb_batch_size": (C.c_int, [C.c_void_p]),
@@ -480,6 +482,16 @@ class SGN2DB200:
         _check(lib().sgnb_sample_eta(self._h, nd.ctypes.data_as(C.POINTER(C.c_longlong)),
                                      int(nd.size), _ptr(out)), self._h)
         return out
+
+    def element_means(self):
+        """Element means of (eta, u, v, p, H), shape [5, Ny, Nx]."""
+        out = np.zeros(5 * self.Nx * self.Ny)
+        _check(lib().sgnb_element_means(self._h, _ptr(out)), self._h)
+        return out.reshape(5, self.Ny, self.Nx)
+
+    def write_vtk(self, path):
+        """Legacy-VTK frame of the element means (the reference's vtk2d.h format)."""
+        _check(lib().sgnb_write_vtk(self._h, os.fsencode(path)), self._h)
 
     def nearest_node(self, x, y):
         n = C.c_longlong()
