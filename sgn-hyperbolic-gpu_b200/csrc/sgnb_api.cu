@@ -947,6 +947,8 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
       return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run in SGNB_FP64_FAST or SGNB_MIXED");
     if (descs[i].precision != descs[0].precision)
       return bfail(nullptr, SGNB_ERR_INVALID, "all instances of a batch in one arithmetic mode");
+    if (descs[i].nManning != 0.0)
+      return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run without Manning friction");
     if (descs[i].device != descs[0].device)
       return bfail(nullptr, SGNB_ERR_INVALID, "all instances on one device");
   }

@@ -392,7 +392,7 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 // One tile of the fused right-hand side / stage kernel: tile (bx, by) of the mesh whose
 // constants are C, error partial slot blk. Shared by the single-instance kernel and the
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
-template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA>
+template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false>
 __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_>::Smem& S) {
@@ -575,6 +575,14 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       // round 2: 2/9 k1 + 1/3 k2 in place, k3 into the G area while u comes through
       // registers, then uNew = u + dt ((2/9 k1 + 1/3 k2) + 4/9 k3) (rk.cpp:106-108),
       // written to shared memory and out as the candidate state
+      // every u load of the tile is issued first, so that they are in flight together
+      // with the k3 copies (one memory round trip for the round, not one per field)
+      double ux[NV][NIT];
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int u = 0; u < NIT; ++u)
+          if (okk[u]) ux[v][u] = I.u[(long long)v * Nd + gof[u]];
 #pragma unroll
       for (int v = 0; v < NV; ++v)
 #pragma unroll
@@ -585,18 +593,14 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             cp_async8(&(&S.G[v][0][0])[sof[u]], I.k3 + (long long)v * Nd + gof[u]);
           }
       double* __restrict__ unew = A.U[cur ^ 1];
+      cp_async_wait_all();
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        double x[NIT];
-#pragma unroll
-        for (int u = 0; u < NIT; ++u)
-          if (okk[u]) x[u] = I.u[(long long)v * Nd + gof[u]];
-        if (v == 0) cp_async_wait_all();
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
             double& y = (&S.U[v][0][0])[sof[u]];
-            const double un = fsal_finish(x[u], y, (&S.G[v][0][0])[sof[u]], I.dt);
+            const double un = fsal_finish(ux[v][u], y, (&S.G[v][0][0])[sof[u]], I.dt);
             y = un;
             unew[(long long)v * Nd + gof[u]] = un;
           }
@@ -700,7 +704,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             const double bath = C.g * (Un[a][0] - Hn[a]) + C.gamma * q.p;
             double Sv = bath * (v == 1 ? depth_grad<EXACT, 0>(C, Tb, S.H[i], a, j)
                                        : depth_grad<EXACT, 1>(C, Tb, S.H[i], a, j));
-            if (C.manning) {
+            if constexpr (FRIC) {
               // Manning friction along the velocity, n^2 g |vel| vel / h^(1/3)
               // (sgn_flux2d.h:135-142)
               const double vmag = sqrt(q.u * q.u + q.v * q.v);
@@ -826,12 +830,14 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 }
 
 
-template <int MODE, bool EXACT>
+// FRIC: Manning friction compiled in (instantiated only for contexts that use it, so the
+// frictionless kernels carry none of its code).
+template <int MODE, bool EXACT, bool FRIC = false>
 __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using T = Tile<8, 4>;
   T::Smem& S = *reinterpret_cast<T::Smem*>(smem_raw);
-  fused_tile<MODE, EXACT, 8, 4>(C, C, A, blockIdx.x, blockIdx.y,
+  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC>(C, C, A, blockIdx.x, blockIdx.y,
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 

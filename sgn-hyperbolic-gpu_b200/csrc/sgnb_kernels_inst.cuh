@@ -11,21 +11,29 @@ namespace dev {
 template <int MODE>
 static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
   const dim3 grid((C.Nx + 7) / 8, (C.Ny + 3) / 4);
-  k_fused<MODE, SGNB_EXACT><<<grid, NTHR, sizeof(Tile<8, 4>::Smem), s>>>(C, A);
+  const size_t smem = sizeof(Tile<8, 4>::Smem);
+  if (C.manning) k_fused<MODE, SGNB_EXACT, true><<<grid, NTHR, smem, s>>>(C, A);
+  else k_fused<MODE, SGNB_EXACT, false><<<grid, NTHR, smem, s>>>(C, A);
   return cudaGetLastError();
 }
 
-static cudaError_t prepare_all() {
+template <bool FRIC>
+static cudaError_t prepare_fric() {
   const int bytes = (int)sizeof(Tile<8, 4>::Smem);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT>,
+  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+static cudaError_t prepare_all() {
+  cudaError_t e = prepare_fric<false>();
+  return e == cudaSuccess ? prepare_fric<true>() : e;
 }
 
 static cudaError_t launch_any(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {

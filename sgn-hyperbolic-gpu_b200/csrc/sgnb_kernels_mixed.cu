@@ -8,7 +8,8 @@ namespace dev {
 template <int MODE>
 static cudaError_t launch_m(const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
   const dim3 grid((C.Nx + mix::TX - 1) / mix::TX, (C.Ny + mix::TY - 1) / mix::TY);
-  mix::k_mixed<MODE><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  if (C.manning) mix::k_mixed<MODE, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  else mix::k_mixed<MODE, false><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
   return cudaGetLastError();
 }
 
@@ -21,17 +22,23 @@ cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A
   }
 }
 
-cudaError_t prepare_fused_mixed() {
+template <bool FRIC>
+static cudaError_t prepare_mixed_fric() {
   const int bytes = (int)sizeof(mix::Smem);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_RHS>,
+  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_RHS, FRIC>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_STAGE>,
+  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_STAGE, FRIC>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(mix::k_mixed<mix::MODE_FSAL>,
+  return cudaFuncSetAttribute(mix::k_mixed<mix::MODE_FSAL, FRIC>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t prepare_fused_mixed() {
+  cudaError_t e = prepare_mixed_fric<false>();
+  return e == cudaSuccess ? prepare_mixed_fric<true>() : e;
 }
 
 template <int MODE>

@@ -225,7 +225,7 @@ __device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const doub
 
 // One tile (bx, by) of the mixed-precision right-hand side / stage kernel, error partial
 // slot blk. Shared by the single-instance kernel and the batched kernel.
-template <int MODE, class TC, class TB, class TA>
+template <int MODE, class TC, class TB, class TA, bool FRIC = false>
 __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& A, int bx, int by,
                                            long long blk, Smem& S) {
 
@@ -512,7 +512,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           } else if (v == 1 || v == 2) {
             // Manning friction n^2 g |vel| vel / h^(1/3), a deviation term (FP32)
             float fr = 0.0f;
-            if (C.manning)
+            if constexpr (FRIC)
               fr = (float)C.n2g * sqrtf(s.u * s.u + s.v * s.v) / cbrtf(s.h) *
                    (v == 1 ? s.u : s.v);
             res = v == 1 ? hydu[a] + gammaf * s.p * Hxf[a] - fr - (d + g)
@@ -629,12 +629,12 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   }
 }
 
-template <int MODE>
+template <int MODE, bool FRIC = false>
 __global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const StageArgsM A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
-  mixed_tile<MODE>(C, C, A, blockIdx.x, blockIdx.y,
-                   (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
+  mixed_tile<MODE, RhsConsts, RhsConsts, StageArgsM, FRIC>(
+      C, C, A, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
 // Batched form (8x4 tiles): the work list of BatchArgsM, per tile the instance's constants
