@@ -58,7 +58,7 @@ enum : int {
 };
 
 // A tile of TX x TY = 32 elements (TX in 4, 8, 16) and its shared-memory layout.
-template <int TX_, int TY_>
+template <int TX_, int TY_, bool EXACT_ = false>
 struct Tile {
   static constexpr int TX = TX_, TY = TY_;
   static_assert(TX * TY == TE, "one tile element per lane");
@@ -70,7 +70,9 @@ struct Tile {
   struct Smem {
     double U[NV][TE][NPP];       // tile state (input of R)
     double H[TE][NPP];           // nodal still depth (its gradient is formed from it)
-    double G[NV + 1][TE][NPP];   // column-pass results dG (5 fields) and By; then dU
+    // column-pass results dG (5 fields) and, in the exact mode, By on its own (the fast
+    // mode adds By to the hp field's dG); then dU
+    double G[NV + (EXACT_ ? 1 : 0)][TE][NPP];
     // halo node states, flat index q = t + NP * (slot + NHALO * v):
     //   slot 0..TY-1        node (4,t) of the element left of tile row slot
     //   slot TY..2TY-1      node (0,t) of the element right of tile row slot-TY
@@ -395,8 +397,8 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false>
 __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
-                                           typename Tile<TX_, TY_>::Smem& S) {
-  using T = Tile<TX_, TY_>;
+                                           typename Tile<TX_, TY_, EXACT>::Smem& S) {
+  using T = Tile<TX_, TY_, EXACT>;
   constexpr int TX = T::TX, TY = T::TY, NHALO = T::NHALO, RUN = T::RUN;
   constexpr int NHIT = T::NHIT, NFACE = T::NFACE, NFIT = T::NFIT;
 
@@ -644,12 +646,17 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     }
     const double HfLo = T::hf_y(S, i, j);
     const double HfHi = (iy + 1 < TYv) ? T::hf_y(S, i + TX, j) : T::hf_yt(S, ix, j);
+    double by[NP];  // ncpY, -c^2 v h_y (sgn_flux2d.h:156-161)
     line_pass<EXACT, 1>(
         C, Tb, Un, Hn, nLo, nHi, HfLo, HfHi,
         [&](int b, double dh, const Prim<EXACT>& q) {
-          S.G[NV][i][j + NP * b] = C.mc2 * q.v * dh;  // ncpY (sgn_flux2d.h:156-161)
+          if constexpr (EXACT) S.G[NV][i][j + NP * b] = C.mc2 * q.v * dh;
+          else by[b] = C.mc2 * q.v * dh;
         },
-        [&](int b, int v, double d, const Prim<EXACT>&) { S.G[v][i][j + NP * b] = d; });
+        [&](int b, int v, double d, const Prim<EXACT>&) {
+          if constexpr (EXACT) S.G[v][i][j + NP * b] = d;
+          else S.G[v][i][j + NP * b] = v == NV - 1 ? d + by[b] : d;
+        });
   }
   __syncthreads();
 
@@ -717,8 +724,12 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             const double Hyl = depth_grad<EXACT, 1>(C, Tb, S.H[i], a, j);
             const double S4 = C.m2c2 * (q.w + q.u * Hxl + q.v * Hyl);
             const double Bx = C.mc2 * q.u * dhx[a];  // ncpX (sgn_flux2d.h:150-155)
-            const double By = S.G[NV][i][loc];
-            res = EXACT ? (((-d - g) - Bx) - By) + S4 : S4 - (d + g) - Bx - By;
+            if constexpr (EXACT) {
+              const double By = S.G[NV][i][loc];
+              res = (((-d - g) - Bx) - By) + S4;
+            } else {
+              res = S4 - (d + g) - Bx;  // g holds dG + By
+            }
           }
           S.G[v][i][loc] = res;
         });
@@ -835,8 +846,8 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 template <int MODE, bool EXACT, bool FRIC = false>
 __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  using T = Tile<8, 4>;
-  T::Smem& S = *reinterpret_cast<T::Smem*>(smem_raw);
+  using T = Tile<8, 4, EXACT>;
+  typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
   fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC>(C, C, A, blockIdx.x, blockIdx.y,
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
@@ -849,7 +860,7 @@ __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(
 // to the next, which the loop costs in spilled registers).
 template <int MODE, bool EXACT, int TX_, int TY_>
 __device__ __forceinline__ void batch_tile(const BatchArgs& B, long long t,
-                                           typename Tile<TX_, TY_>::Smem& S, RhsConsts& Cs,
+                                           typename Tile<TX_, TY_, EXACT>::Smem& S, RhsConsts& Cs,
                                            StageArgs& As) {
   const int inst = B.tile_inst[t];
   const long long lt = t - B.tile_start[inst];
@@ -882,7 +893,7 @@ __global__ void __launch_bounds__(NTHR, 2) k_fused_batch(const BatchArgs B) {
   // FR tables come from the kernel parameters (constant bank): the same for every
   // instance (P = 4 GLL)
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  using T = Tile<TX_, TY_>;
+  using T = Tile<TX_, TY_, EXACT>;
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
   __shared__ RhsConsts Cs;
   __shared__ StageArgs As;

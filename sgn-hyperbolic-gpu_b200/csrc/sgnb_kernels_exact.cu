@@ -11,6 +11,6 @@ cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
 }
 cudaError_t prepare_fused_exact() { return prepare_all(); }
 int fused_grid_blocks(int Nx, int Ny) { return ((Nx + 7) / 8) * ((Ny + 3) / 4); }
-size_t fused_smem_bytes() { return sizeof(Tile<8, 4>::Smem); }
+size_t fused_smem_bytes() { return sizeof(Tile<8, 4, true>::Smem); }
 }  // namespace dev
 }  // namespace sgnb

@@ -13,7 +13,7 @@ cudaError_t prepare_fused_fast() { return prepare_all(); }
 
 template <int MODE, int TXs, int TYs>
 static cudaError_t launch_b(int blocks, const BatchArgs& B, cudaStream_t s) {
-  const size_t smem = sizeof(typename Tile<TXs, TYs>::Smem);
+  const size_t smem = sizeof(typename Tile<TXs, TYs, false>::Smem);
   if (blocks > 0) {
     k_fused_batch<MODE, false, TXs, TYs, true><<<blocks, NTHR, smem, s>>>(B);
   } else {
@@ -47,7 +47,7 @@ int batch_tile_tx(int shape_id) { return shape_id == 1 ? 16 : (shape_id == 2 ? 4
 
 template <int MODE, int TXs, int TYs>
 static cudaError_t prepare_mode() {
-  const int bytes = (int)sizeof(typename Tile<TXs, TYs>::Smem);
+  const int bytes = (int)sizeof(typename Tile<TXs, TYs, false>::Smem);
   cudaError_t e = cudaFuncSetAttribute(k_fused_batch<MODE, false, TXs, TYs, true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;

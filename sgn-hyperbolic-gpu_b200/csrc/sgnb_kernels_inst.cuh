@@ -11,7 +11,7 @@ namespace dev {
 template <int MODE>
 static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
   const dim3 grid((C.Nx + 7) / 8, (C.Ny + 3) / 4);
-  const size_t smem = sizeof(Tile<8, 4>::Smem);
+  const size_t smem = sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
   if (C.manning) k_fused<MODE, SGNB_EXACT, true><<<grid, NTHR, smem, s>>>(C, A);
   else k_fused<MODE, SGNB_EXACT, false><<<grid, NTHR, smem, s>>>(C, A);
   return cudaGetLastError();
@@ -19,7 +19,7 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
 
 template <bool FRIC>
 static cudaError_t prepare_fric() {
-  const int bytes = (int)sizeof(Tile<8, 4>::Smem);
+  const int bytes = (int)sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
