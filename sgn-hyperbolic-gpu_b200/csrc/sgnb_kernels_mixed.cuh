@@ -74,16 +74,26 @@ struct StageInM {
   double acoef, dt;
 };
 
-// FP64 stage input (src/solver/rk.cpp:100-108 with FP32 derivatives promoted).
+// FP64 stage combinations (src/solver/rk.cpp:100-108 with FP32 derivatives promoted),
+// every product and sum rounded on its own: a tile forms its own nodes and its
+// neighbours' halo nodes in different code, and the two must agree bit for bit.
+__device__ __forceinline__ double stage_m(double u, double acoef, float k) {
+  return __dadd_rn(u, __dmul_rn(acoef, (double)k));
+}
+__device__ __forceinline__ double fsal_m(double u, float k1, float k2, float k3, double dt) {
+  const double s = __dadd_rn(__dadd_rn(__dmul_rn(2.0 / 9.0, (double)k1), __dmul_rn(1.0 / 3.0, (double)k2)),
+                             __dmul_rn(4.0 / 9.0, (double)k3));
+  return __dadd_rn(u, __dmul_rn(dt, s));
+}
+
 template <int MODE>
 __device__ __forceinline__ double stage_value(const StageInM& I, long long idx) {
   if constexpr (MODE == MODE_RHS) {
     return I.in[idx];
   } else if constexpr (MODE == MODE_STAGE) {
-    return I.u[idx] + I.acoef * (double)I.k[idx];
+    return stage_m(I.u[idx], I.acoef, I.k[idx]);
   } else {
-    return I.u[idx] + I.dt * (2.0 / 9.0 * (double)I.k1[idx] + 1.0 / 3.0 * (double)I.k2[idx] +
-                              4.0 / 9.0 * (double)I.k3[idx]);
+    return fsal_m(I.u[idx], I.k1[idx], I.k2[idx], I.k3[idx], I.dt);
   }
 }
 
@@ -295,16 +305,40 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
                          "l"(I.k + (long long)v * Nd + gof[u]) : "memory");
           }
     }
-    // stage mode: every u load of the tile in flight before the first combination
+    // end-point stage: k1 and k2 by asynchronous copies into the (still unused) G and q
+    // areas, ten FP32 fields
+    auto k12_slot = [&](int w, int v) -> float* {  // w: 0 = k1, 1 = k2
+      const int f = 5 * w + v;                     // G[0..5] then q[0..3]
+      return f < NV + 1 ? &S.G[f][0][0] : &S.q[f - NV - 1][0][0];
+    };
+    if constexpr (MODE == MODE_FSAL) {
+#pragma unroll
+      for (int w = 0; w < 2; ++w)
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+          for (int u = 0; u < NIT; ++u)
+            if (okk[u]) {
+              const unsigned sa = (unsigned)__cvta_generic_to_shared(k12_slot(w, v) + sof[u]);
+              asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
+                           "l"((w == 0 ? I.k1 : I.k2) + (long long)v * Nd + gof[u]) : "memory");
+            }
+    }
+    // every u load (and, at the end point, every k3 load) of the tile in flight before the
+    // first combination
     double ux[NV][NIT];
-    if constexpr (MODE == MODE_STAGE) {
+    float k3x[NV][NIT];
+    if constexpr (MODE != MODE_RHS) {
 #pragma unroll
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u]) ux[v][u] = I.u[(long long)v * Nd + gof[u]];
+          if (okk[u]) {
+            ux[v][u] = I.u[(long long)v * Nd + gof[u]];
+            if constexpr (MODE == MODE_FSAL) k3x[v][u] = I.k3[(long long)v * Nd + gof[u]];
+          }
+      cp_async_wait_all();  // k (k1, k2) and the statics have landed
     }
-    if constexpr (MODE == MODE_STAGE) cp_async_wait_all();  // k and the statics have landed
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       double x[NIT];
@@ -312,7 +346,10 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           if constexpr (MODE == MODE_STAGE)
-            x[u] = ux[v][u] + I.acoef * (double)(&S.G[v][0][0])[sof[u]];
+            x[u] = stage_m(ux[v][u], I.acoef, (&S.G[v][0][0])[sof[u]]);
+          else if constexpr (MODE == MODE_FSAL)
+            x[u] = fsal_m(ux[v][u], k12_slot(0, v)[sof[u]], k12_slot(1, v)[sof[u]], k3x[v][u],
+                          I.dt);
           else
             x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
         }
