@@ -52,6 +52,16 @@ def build() -> None:
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
+def reference_rhs_1d(P, N, L, g, c, gamma, U1):
+    """The reference's 1D solver's right-hand side (flat bottom, periodic), var-major
+    (h, hu, hw, hp); needs the compiled reference."""
+    lib = _load(LIB_REFERENCE)
+    U1 = np.ascontiguousarray(U1, dtype=np.float64)
+    out = np.empty_like(U1)
+    lib.or_rhs_1d(P, N, L, g, c, gamma, _ptr(U1), _ptr(out))
+    return out
+
+
 def reference_available() -> bool:
     return os.path.exists(LIB_REFERENCE)
 
@@ -74,6 +84,10 @@ def _load(path: str) -> C.CDLL:
     lib.or_ndof.argtypes = [C.c_void_p]
     lib.or_tables.argtypes = [C.c_void_p] + [_dp] * 7
     lib.or_bathymetry.argtypes = [C.c_void_p] + [_dp] * 7
+    if hasattr(lib, "or_rhs_1d"):
+        lib.or_rhs_1d.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, _dp, _dp]
+        lib.or_rhs_1d.restype = C.c_int
     if hasattr(lib, "or_write_vtk"):
         lib.or_write_vtk.argtypes = [C.c_void_p, _dp, C.c_char_p]
         lib.or_write_vtk.restype = C.c_int

@@ -15,6 +15,7 @@
 #include "or_bathy.h"
 
 #include "solver/rk.h"
+#include "solver/sgn1d.h"
 #include "solver/sgn2d.h"
 #include "io/vtk2d.h"
 
@@ -116,6 +117,21 @@ or_ctx* or_create(int P, int Nx, int Ny, double Lx, double Ly, double g, double 
 }
 
 void or_destroy(or_ctx* s) { delete s; }
+
+/* [reference only] the reference's 1D solver (src/solver/sgn1d.h:47-94) on N periodic
+ * elements of length L with a flat bottom: dU1 = R1(U1), var-major (h, hu, hw, hp),
+ * (P + 1) N nodes per field. The 2D <-> 1D embedding gates of test/test_sgn2d.cpp:79-157
+ * compare the 2D right-hand side of x- or y-invariant states with it. Returns 0. */
+int or_rhs_1d(int P, int N, double L, double g, double c, double gamma, const double* U1,
+              double* dU1) {
+  sgn::Params par;
+  par.g = g; par.c = c; par.gamma = gamma;
+  sgn::SGN1D s1(P, N, L, par);
+  sgn::State U(U1, U1 + (size_t)s1.nTotal()), R;
+  s1.rhs(U, R);
+  std::memcpy(dU1, R.data(), R.size() * sizeof(double));
+  return 0;
+}
 
 /* [reference only] the reference's VTK frame writer (src/io/vtk2d.h) on a periodic
  * domain; returns 0, or -1 when the domain has walls (mirror doubling would write the

@@ -179,3 +179,41 @@ def test_translation_equivariance_full_size():
             assert torch.equal(torch.roll(R, shifts=(3, 5), dims=(1, 2)), Rs)
             assert torch.isfinite(R).all()
     assert Nd == U[0].numel()
+
+
+@pytest.mark.parametrize("axis", ["x", "y"])
+@pytest.mark.parametrize("prec", [sgnb.FP64_EXACT, sgnb.FP64_FAST])
+def test_embedding_vs_reference_1d(need_reference, axis, prec):
+    """The 2D <-> 1D embedding gates of the reference (test/test_sgn2d.cpp:79-157): an x-
+    (or y-) invariant state over a flat bottom, with the transverse velocity zero, gives on
+    every line the reference 1D solver's right-hand side (within 1e-12, the reference's
+    gate) and a zero transverse-momentum right-hand side."""
+    from cases import G, gll5, make_state, node_coords
+
+    P, Nx, Ny, Lx, Ly, H0 = 4, 8, 6, 10.0, 8.0, 1.0
+    c = 3.0 * np.sqrt(G * H0)
+    x, y = node_coords(P, Nx, Ny, Lx, Ly, gll5())
+    s, L = (x, Lx) if axis == "x" else (y, Ly)
+    k = 2 * np.pi / L
+    h = H0 + 0.08 * np.sin(k * s)
+    un = 0.15 * np.cos(k * s)
+    z = np.zeros_like(s)
+    U2 = make_state(h, un, z, 0.04 * np.sin(k * s), 0.02 * np.cos(k * s)) if axis == "x" else \
+        make_state(h, z, un, 0.04 * np.sin(k * s), 0.02 * np.cos(k * s))
+    with sgnb.SGN2DB200(P=P, Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, c=c, precision=prec) as d:
+        R2 = d.rhs(U2).reshape(5, Ny, Nx, 5, 5)  # [v, ey, ex, b, a]
+    nd, td = (1, 2) if axis == "x" else (2, 1)
+    # the 1D state: the 2D state along the line ey = 0, b = 0 (x) or ex = 0, a = 0 (y)
+    U2r = U2.reshape(5, Ny, Nx, 5, 5)
+    line = (lambda A: A[:, 0, :, 0, :].reshape(A.shape[0], -1)) if axis == "x" else \
+        (lambda A: A[:, :, 0, :, 0].reshape(A.shape[0], -1))
+    N = Nx if axis == "x" else Ny
+    U1 = np.concatenate([line(U2r)[v] for v in (0, nd, 3, 4)])
+    R1 = O.reference_rhs_1d(P, N, L, G, c, 1.5, U1).reshape(4, -1)
+    R2l = line(R2)
+    err = max(np.abs(R2l[v2] - R1[v1]).max() for v1, v2 in enumerate((0, nd, 3, 4)))
+    assert err < 1e-12, err
+    assert np.abs(R2[td]).max() < 1e-12
+    # every line is the same line
+    lines = R2[(0, nd, 3, 4), :, :, 0, :] if axis == "x" else R2[(0, nd, 3, 4), :, :, :, 0]
+    assert np.abs(lines - lines[:, :1] if axis == "x" else lines - lines[:, :, :1]).max() < 1e-12
