@@ -67,7 +67,7 @@ enum {
 typedef struct {
   int P, Nx, Ny;             /* only P = 4 is built; Nx, Ny >= 2 */
   double Lx, Ly;
-  double g, c, gamma, nManning; /* nManning must be 0 (Manning friction is not built) */
+  double g, c, gamma, nManning; /* nManning >= 0: Manning friction (0 = off) */
   int bc_x, bc_y;            /* SGNB_BC_*; walls are an addition to the reference */
   int precision;             /* SGNB_FP64_EXACT, SGNB_FP64_FAST or SGNB_MIXED */
   int device;                /* CUDA device ordinal */
@@ -80,6 +80,11 @@ typedef struct {
    * (sgn2d.h:94-98; Nd, Nd, Nd, 5 Nx Ny, 5 Nx Ny doubles) and, for walls, the depth on
    * the right edge (5 Ny, sampled at x = Nx hx) and top edge (5 Nx, at y = Ny hy). */
   const double *Hnod, *Hx, *Hy, *HfaceX, *HfaceY, *HfaceXEnd, *HfaceYEnd;
+  /* Slab of a larger mesh (x decomposition, as the reference's multi-GPU solver splits
+   * it, src/parallel/slab1d.h:55-72): the full mesh has Nx_global elements over Lx and
+   * this context owns the Nx columns from ex_offset on; node coordinates, bathymetry and
+   * face depths are the full mesh's. Nx_global = 0: the context is the whole mesh. */
+  int Nx_global, ex_offset;
 } sgnb_desc;
 
 /* AdaptiveRKOptions (src/solver/rk.h:53-61). */
@@ -197,6 +202,39 @@ int sgnb_fr_tables(int P, double* nodes, double* D, double* lL, double* lR, doub
 int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* Hy,
                           double* HfaceX, double* HfaceY, double* HfaceXEnd,
                           double* HfaceYEnd);
+
+/* Slab decomposition (the reference's multi-GPU solver, src/cuda/sgn2d_cuda_mpi.cu:148-161,
+ * 487-537: x slabs, one halo exchange per right-hand side, one reduction of the error norm
+ * per step). A slab is a context created with Nx_global / ex_offset; its neighbours'
+ * traces across the slab edges come from ghost arrays [5 fields][Ny][5 nodes] that the
+ * caller fills with the neighbours' packed edges before every stage; the caller gathers
+ * every slab's error partials and runs each slab's controller on all of them, so that
+ * every slab takes the same decision.
+ *   sgnb_set_ghosts   device ghost arrays of the left / right edge (NULL: the edge
+ *                     follows bc_x: a wall, or the periodic wrap of a single slab)
+ *   sgnb_slab_pack    this slab's edge nodes for the neighbours: stage 0 = the input
+ *                     `in` of a right-hand side (NULL: the current state), 2 / 3 = the
+ *                     intermediate stages of the running attempt, 4 = its end-point
+ *                     candidate; sendL / sendR are [5][Ny][5] device arrays
+ *   sgnb_slab_begin   the controller for nsteps accepted steps from dt0 (dts != NULL:
+ *                     frozen step sizes, the bs3Step replay)
+ *   sgnb_slab_launch  stage 1 (FSAL head k1 = R(u)), 2, 3, 4 (end point, error partials)
+ *   sgnb_slab_partials / sgnb_slab_control / sgnb_slab_status: this slab's partials
+ *                     (3 doubles per tile), the controller on the gathered partials of all
+ *                     slabs (n_total = 5 x the nodes of the whole mesh), the controller
+ *                     state (synchronises).
+ * The right-hand side of a slab is sgnb_rhs_device after its ghosts hold the neighbours'
+ * packed inputs. FP64 modes; `stream` NULL = the context's stream. */
+int sgnb_set_ghosts(sgnb_ctx* ctx, const double* ghostL, const double* ghostR);
+int sgnb_slab_pack(sgnb_ctx* ctx, int stage, const double* in, double* sendL, double* sendR,
+                   void* stream);
+int sgnb_slab_begin(sgnb_ctx* ctx, double t0, double dt0, long long nsteps, const double* dts,
+                    const sgnb_rk_opts* opts);
+int sgnb_slab_launch(sgnb_ctx* ctx, int stage, void* stream);
+int sgnb_slab_partials(sgnb_ctx* ctx, double** partials, int* nblk);
+int sgnb_slab_control(sgnb_ctx* ctx, const double* partials, int nblk, long long n_total,
+                      void* stream);
+int sgnb_slab_status(sgnb_ctx* ctx, sgnb_rk_stats* st, int* done, void* stream);
 
 /* Device-side sampling for the reference's applications, which download the whole state
  * at every sample time and scan it on the host (apps/shoal_focus_mpi.cu:195-205,

@@ -176,6 +176,8 @@ int sgnb_adj_create(sgnb_ctx* c, long long nsteps, const double* dts, int ngauge
     return afail(c, SGNB_ERR_INVALID, "sgnb_adj_create: bad arguments");
   *out = nullptr;
   if (c->mixed) return afail(c, SGNB_ERR_UNSUPPORTED, "the adjoint runs in FP64 modes");
+  if (c->desc.Nx_global > 0 || c->C.ghostL || c->C.ghostR)
+    return afail(c, SGNB_ERR_UNSUPPORTED, "the adjoint runs on whole meshes");
   for (int g = 0; g < ngauges; ++g)
     if (gauge_nodes[g] < 0 || gauge_nodes[g] >= c->Nd)
       return afail(c, SGNB_ERR_INVALID, "gauge node out of range");

@@ -104,6 +104,8 @@ int check_desc(const sgnb_desc* d) {
   if (d->precision != SGNB_FP64_EXACT && d->precision != SGNB_FP64_FAST &&
       d->precision != SGNB_MIXED)
     return fail(nullptr, SGNB_ERR_UNSUPPORTED, "unknown precision mode");
+  if (d->Nx_global < 0 || (d->Nx_global > 0 && (d->ex_offset < 0 || d->ex_offset + d->Nx > d->Nx_global)))
+    return fail(nullptr, SGNB_ERR_INVALID, "slab: 0 <= ex_offset, ex_offset + Nx <= Nx_global");
   if ((long long)d->Nx * d->Ny > (1ll << 31) / 25)
     return fail(nullptr, SGNB_ERR_INVALID, "mesh too large");
   if (d->bathy_kind == SGNB_BATHY_ARRAYS) {
@@ -142,7 +144,9 @@ int tables_for(const sgnb_desc* d, FrTables& t) {
 Mesh mesh_for(const sgnb_desc* d) {
   Mesh m;
   m.Nx = d->Nx; m.Ny = d->Ny; m.Lx = d->Lx; m.Ly = d->Ly;
-  m.hx = d->Lx / d->Nx; m.hy = d->Ly / d->Ny;  // mesh2d.h:27-28
+  m.hx = d->Lx / (d->Nx_global > 0 ? d->Nx_global : d->Nx); m.hy = d->Ly / d->Ny;  // mesh2d.h:27-28
+  m.ex0 = d->Nx_global > 0 ? d->ex_offset : 0;
+  m.wrapx = d->Nx_global > 0 && d->bc_x == SGNB_BC_PERIODIC && d->ex_offset + d->Nx == d->Nx_global;
   return m;
 }
 
@@ -478,6 +482,8 @@ int sgnb_rhs_host(sgnb_ctx* c, const double* U, double* dU) {
 int sgnb_integrate_adaptive(sgnb_ctx* c, double t0, double tEnd, double dt0,
                             const sgnb_rk_opts* opts, sgnb_rk_stats* st) {
   if (!c) return fail(c, SGNB_ERR_INVALID, "NULL context");
+  if (c->C.ghostL || c->C.ghostR)
+    return fail(c, SGNB_ERR_INVALID, "a slab integrates through the slab entries (sgnb_slab_*)");
   if (int rc = set_device(c)) return rc;
   sgnb_rk_opts o;
   if (opts) o = *opts; else sgnb_rk_opts_init(&o);
@@ -539,6 +545,8 @@ int sgnb_launch_stage(sgnb_ctx* c, int stage, double dt, int count, void* stream
 
 int sgnb_bs3_steps(sgnb_ctx* c, double t0, const double* dts, long long n) {
   if (!c || (n > 0 && !dts) || n < 0) return fail(c, SGNB_ERR_INVALID, "bad arguments");
+  if (c->C.ghostL || c->C.ghostR)
+    return fail(c, SGNB_ERR_INVALID, "a slab integrates through the slab entries (sgnb_slab_*)");
   if (n == 0) return SGNB_OK;
   if (int rc = set_device(c)) return rc;
   if (n > c->dtCap) {
@@ -831,13 +839,128 @@ int batch_run(sgnb_batch* b) {
 
 extern "C" {
 
+int sgnb_set_ghosts(sgnb_ctx* c, const double* ghostL, const double* ghostR) {
+  if (!c) return fail(c, SGNB_ERR_INVALID, "NULL context");
+  if (c->mixed) return fail(c, SGNB_ERR_UNSUPPORTED, "slab edges run in the FP64 modes");
+  c->C.ghostL = ghostL;
+  c->C.ghostR = ghostR;
+  if (c->chunk) {  // captured launches hold the old constants
+    cudaGraphExecDestroy(c->chunk);
+    c->chunk = nullptr;
+    c->chunkLen = 0;
+  }
+  return SGNB_OK;
+}
+
+int sgnb_slab_pack(sgnb_ctx* c, int stage, const double* in, double* sendL, double* sendR,
+                   void* stream) {
+  if (!c || !sendL || !sendR || !(stage == 0 || stage == 2 || stage == 3 || stage == 4))
+    return fail(c, SGNB_ERR_INVALID, "stage 0, 2, 3 or 4; send buffers");
+  if (c->mixed) return fail(c, SGNB_ERR_UNSUPPORTED, "slab edges run in the FP64 modes");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  StageArgs A{};
+  A.U[0] = c->U[0]; A.U[1] = c->U[1];
+  A.K1[0] = (double*)c->K1[0]; A.K1[1] = (double*)c->K1[1];
+  A.K2 = (double*)c->K2; A.K3 = (double*)c->K3;
+  A.ctrl = c->dctrl;
+  A.in = in ? in : c->U[c->cur];
+  A.kin_k2 = stage == 3;
+  A.coef = stage == 3 ? 0.75 : 0.5;
+  const int mode = stage == 0 ? 0 : (stage == 4 ? 2 : 1);
+  SGNB_CU(c, dev::launch_pack_ghosts(mode, c->C, A, sendL, sendR, s));
+  return SGNB_OK;
+}
+
+int sgnb_slab_begin(sgnb_ctx* c, double t0, double dt0, long long nsteps, const double* dts,
+                    const sgnb_rk_opts* opts) {
+  if (!c || nsteps < 1 || !(dt0 > 0)) return fail(c, SGNB_ERR_INVALID, "nsteps >= 1, dt0 > 0");
+  if (int rc = set_device(c)) return rc;
+  sgnb_rk_opts o;
+  if (opts) o = *opts; else sgnb_rk_opts_init(&o);
+  CtrlState& h = *c->hctrl;
+  init_ctrl(c, h, o);
+  h.log = nullptr;
+  h.t = t0;
+  h.tEnd = 1e300;
+  h.dt = (o.dtMax < dt0) ? o.dtMax : dt0;
+  h.errPrev = 1.0;
+  h.tReached = t0;
+  h.cur = c->cur;
+  h.rhsEvals = 1;  // the FSAL head
+  h.maxAccepted = nsteps;
+  if (dts) {  // frozen step sizes (bs3Step replay)
+    if (nsteps > c->dtCap) {
+      cudaFree(c->dtList);
+      c->dtList = nullptr;
+      SGNB_CU(c, cudaMalloc(&c->dtList, nsteps * sizeof(double)));
+      c->dtCap = nsteps;
+    }
+    SGNB_CU(c, cudaMemcpy(c->dtList, dts, nsteps * sizeof(double), cudaMemcpyHostToDevice));
+    h.frozen = 1;
+    h.dtList = c->dtList;
+    h.nList = nsteps;
+    h.dt = dts[0];
+  }
+  SGNB_CU(c, cudaMemcpy(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice));
+  return SGNB_OK;
+}
+
+int sgnb_slab_launch(sgnb_ctx* c, int stage, void* stream) {
+  if (!c || stage < 1 || stage > 4) return fail(c, SGNB_ERR_INVALID, "stage 1..4");
+  if (c->mixed) return fail(c, SGNB_ERR_UNSUPPORTED, "slab edges run in the FP64 modes");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  if (stage == 1)  // FSAL head: k1 = R(u)
+    SGNB_CU(c, launch(c, rhs_launch(c->U[c->cur], (double*)c->K1[c->cur]), s));
+  else
+    SGNB_CU(c, launch(c, stage_launch(stage), s));
+  return SGNB_OK;
+}
+
+int sgnb_slab_partials(sgnb_ctx* c, double** partials, int* nblk) {
+  if (!c || !partials || !nblk) return fail(c, SGNB_ERR_INVALID, "NULL argument");
+  *partials = c->partials;
+  *nblk = c->nblk;
+  return SGNB_OK;
+}
+
+int sgnb_slab_control(sgnb_ctx* c, const double* partials, int nblk, long long n_total,
+                      void* stream) {
+  if (!c || !partials || nblk < 1 || n_total < 1) return fail(c, SGNB_ERR_INVALID, "bad arguments");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  SGNB_CU(c, dev::launch_controller(c->dctrl, partials, nblk, n_total, s));
+  return SGNB_OK;
+}
+
+int sgnb_slab_status(sgnb_ctx* c, sgnb_rk_stats* st, int* done, void* stream) {
+  if (!c) return fail(c, SGNB_ERR_INVALID, "NULL context");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, s));
+  SGNB_CU(c, cudaStreamSynchronize(s));
+  const CtrlState& h = *c->hctrl;
+  c->cur = h.cur;
+  if (done) *done = h.done;
+  if (st) {
+    st->accepted = h.accepted; st->rejected = h.rejected; st->rhsEvals = h.rhsEvals;
+    st->attempts = h.attempts; st->tReached = h.tReached; st->dtLast = h.dtLast;
+    st->maxNormLast = h.maxNormLast;
+    st->aborted = h.done == 2 ? 1 : (h.done == 3 ? 2 : 0);
+    st->status = h.done == 3 ? SGNB_ERR_NAN : SGNB_OK;
+    st->kernel_launches = 0;
+  }
+  return SGNB_OK;
+}
+
 int sgnb_eta_max(sgnb_ctx* c, double x0, double x1, double y0, double y1, double* eta_max,
                  long long* node) {
   if (!c || !eta_max || !node) return fail(c, SGNB_ERR_INVALID, "NULL argument");
   if (int rc = set_device(c)) return rc;
   const int nblk = c->ndiag / 2;
   SGNB_CU(c, dev::launch_eta_max(c->C, c->U[c->cur], x0, x1, y0, y1, c->mesh.hx, c->mesh.hy,
-                                 c->tab.nodes, c->diag, nblk, c->stream));
+                                 c->mesh.ex0, c->tab.nodes, c->diag, nblk, c->stream));
   std::vector<double> part(2 * (size_t)nblk);
   SGNB_CU(c, cudaMemcpyAsync(part.data(), c->diag, part.size() * sizeof(double),
                              cudaMemcpyDeviceToHost, c->stream));
@@ -904,7 +1027,8 @@ int sgnb_write_vtk(sgnb_ctx* c, const char* path) {
   // legacy VTK, one point per element centre (the format of src/io/vtk2d.h:46-82)
   std::fprintf(fp, "# vtk DataFile Version 3.0\nSGN2D element means\nASCII\n");
   std::fprintf(fp, "DATASET STRUCTURED_POINTS\nDIMENSIONS %d %d 1\n", Nx, Ny);
-  std::fprintf(fp, "ORIGIN %.6f %.6f 0\nSPACING %.6f %.6f 1\n", 0.5 * c->mesh.hx,
+  std::fprintf(fp, "ORIGIN %.6f %.6f 0\nSPACING %.6f %.6f 1\n",
+               c->mesh.ex0 * c->mesh.hx + 0.5 * c->mesh.hx,
                0.5 * c->mesh.hy, c->mesh.hx, c->mesh.hy);
   std::fprintf(fp, "POINT_DATA %d\n", Nx * Ny);
   static const char* names[5] = {"eta", "u", "v", "p", "H"};
@@ -929,7 +1053,7 @@ int sgnb_nearest_node(const sgnb_ctx* c, double x, double y, long long* node) {
     const int ex = (int)(e % Nx), ey = (int)(e / Nx);
     for (int b = 0; b < 5; ++b)
       for (int a = 0; a < 5; ++a) {
-        const double xn = ex * c->mesh.hx + 0.5 * c->mesh.hx * (c->tab.nodes[a] + 1.0);
+        const double xn = (c->mesh.ex0 + ex) * c->mesh.hx + 0.5 * c->mesh.hx * (c->tab.nodes[a] + 1.0);
         const double yn = ey * c->mesh.hy + 0.5 * c->mesh.hy * (c->tab.nodes[b] + 1.0);
         const double d2 = (xn - x) * (xn - x) + (yn - y) * (yn - y);
         if (d2 < best) { best = d2; bi = e * 25 + a + 5 * b; }
@@ -949,6 +1073,8 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
       return bfail(nullptr, SGNB_ERR_INVALID, "all instances of a batch in one arithmetic mode");
     if (descs[i].nManning != 0.0)
       return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run without Manning friction");
+    if (descs[i].Nx_global > 0)
+      return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances are whole meshes");
     if (descs[i].device != descs[0].device)
       return bfail(nullptr, SGNB_ERR_INVALID, "all instances on one device");
   }

@@ -33,6 +33,11 @@ struct RhsConsts {
   const double* HfY;     // H at the bottom edge of each element
   const double* HfXEnd;  // H on the right domain edge (walls), 5 per row
   const double* HfYEnd;  // H on the top domain edge (walls), 5 per column
+  // slab edges (x decomposition): the neighbours' trace nodes across the left and right
+  // edge, [field][row][transverse node], stage inputs formed by the neighbours; NULL: the
+  // edge follows bcx (periodic wrap or wall)
+  const double* ghostL;
+  const double* ghostR;
 };
 
 // Device-resident state of the adaptive integrator: the scalar loop variables of
@@ -156,6 +161,12 @@ namespace dev {
 cudaError_t launch_mixed_batch(int mode, int blocks, const BatchArgsM& B, cudaStream_t s);
 cudaError_t prepare_mixed_batch();
 
+// Slab edges: the stage inputs of the first and last element columns' edge nodes
+// (a = 0 / a = 4), [field][row][node], for the neighbours' ghosts. mode 0: rhs of in;
+// 1: intermediate stage (kin_k2, coef of A); 2: end-point candidate.
+cudaError_t launch_pack_ghosts(int mode, const RhsConsts& C, const StageArgs& A, double* sendL,
+                               double* sendR, cudaStream_t s);
+
 // Adjoint kernels (FP64, fast arithmetic).
 cudaError_t launch_vjp_rhs(const RhsConsts& C, const FrTablesDev& T, const VjpArgs& A,
                            const GatherArgs& G, cudaStream_t s);
@@ -195,8 +206,8 @@ cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk,
                               long long n, cudaStream_t s);
 // Largest eta = h - H inside a window, with its node: (value, index) per block.
 cudaError_t launch_eta_max(const RhsConsts& C, const double* U, double x0, double x1, double y0,
-                           double y1, double hx, double hy, const double* xi, double* out,
-                           int nblk, cudaStream_t s);
+                           double y1, double hx, double hy, int ex0, const double* xi,
+                           double* out, int nblk, cudaStream_t s);
 // Element means of eta, u, v, p, H (out[f * ne + e]), as the reference's VTK writer forms them.
 cudaError_t launch_elem_means(const RhsConsts& C, const double* U, const double* qw, double* out,
                               cudaStream_t s);

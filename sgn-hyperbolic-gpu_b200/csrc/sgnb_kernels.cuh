@@ -394,7 +394,8 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 // One tile of the fused right-hand side / stage kernel: tile (bx, by) of the mesh whose
 // constants are C, error partial slot blk. Shared by the single-instance kernel and the
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
-template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false>
+template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false,
+          bool GHOST = false>
 __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_, EXACT>::Smem& S) {
@@ -433,7 +434,13 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
   const long long Nd = C.Nd;
   const int ex0 = bx * TX, ey0 = by * TY;
   const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
-  const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
+  // slab edges: the trace nodes across come from the neighbours' ghost arrays
+  bool ghostL = false, ghostR = false;
+  if constexpr (GHOST) {
+    ghostL = C.ghostL != nullptr && ex0 == 0;
+    ghostR = C.ghostR != nullptr && ex0 + TXv == Nx;
+  }
+  const bool wallL = C.bcx && ex0 == 0 && !ghostL, wallR = C.bcx && ex0 + TXv == Nx && !ghostR;
   const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
 
   // ---- own-node item map: NIT items per thread, shared by every array -------
@@ -491,6 +498,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     // halo items: descriptors, then loads
     double hv[NHIT];
     int hq[NHIT];
+    int hs[NHIT];  // source: 0 the state, 1 the left ghost, 2 the right ghost
     long long hg[NHIT];
 #pragma unroll
     for (int u = 0; u < NHIT; ++u) {
@@ -500,11 +508,14 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       bool ok = q < NV * NHALO * NP;
       long long e = 0;
       int node = 0;
+      hs[u] = 0;
       if (slot < TY) {
+        if (GHOST && ghostL) hs[u] = 1;
         ok = ok && slot < TYv && !wallL;
         e = (long long)((ex0 - 1 + Nx) % Nx) + (long long)Nx * (ey0 + slot);
         node = (NP - 1) + NP * t;
       } else if (slot < 2 * TY) {
+        if (GHOST && ghostR) hs[u] = 2;
         ok = ok && slot - TY < TYv && !wallR;
         e = (long long)((ex0 + TXv) % Nx) + (long long)Nx * (ey0 + slot - TY);
         node = NP * t;
@@ -518,11 +529,17 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
         node = t;
       }
       hq[u] = ok ? q : -1;
-      hg[u] = (long long)v * Nd + e * NPP + node;
+      hg[u] = (GHOST && hs[u]) ? (long long)v * Ny * NP + (long long)(ey0 + (slot < TY ? slot : slot - TY)) * NP + t
+                               : (long long)v * Nd + e * NPP + node;
     }
 #pragma unroll
     for (int u = 0; u < NHIT; ++u)
-      if (hq[u] >= 0) hv[u] = stage_value<MODE>(I, hg[u]);
+      if (hq[u] >= 0) {
+        if constexpr (GHOST)
+          hv[u] = hs[u] == 0 ? stage_value<MODE>(I, hg[u]) : (hs[u] == 1 ? C.ghostL : C.ghostR)[hg[u]];
+        else
+          hv[u] = stage_value<MODE>(I, hg[u]);
+      }
     // face depths
     double fv[NFIT];
     int fq[NFIT];
@@ -544,7 +561,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
         if (slot < TY) {
           if (slot < TYv) {
             const int ey = ey0 + slot;
-            fv[u] = wallR ? C.HfXEnd[(long long)ey * NP + t]
+            fv[u] = (wallR || ghostR) ? C.HfXEnd[(long long)ey * NP + t]
                           : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
             fq[u] = q;
           }
@@ -843,12 +860,13 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 
 // FRIC: Manning friction compiled in (instantiated only for contexts that use it, so the
 // frictionless kernels carry none of its code).
-template <int MODE, bool EXACT, bool FRIC = false>
+// GHOST: slab edges compiled in (only contexts with ghost arrays launch these variants).
+template <int MODE, bool EXACT, bool FRIC = false, bool GHOST = false>
 __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using T = Tile<8, 4, EXACT>;
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
-  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC>(C, C, A, blockIdx.x, blockIdx.y,
+  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC, GHOST>(C, C, A, blockIdx.x, blockIdx.y,
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 

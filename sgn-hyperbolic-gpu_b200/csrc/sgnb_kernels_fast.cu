@@ -11,6 +11,47 @@ cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A, 
 }
 cudaError_t prepare_fused_fast() { return prepare_all(); }
 
+// Slab edges: one thread per (side, field, row, transverse node). Side 0 reads the first
+// element column's left nodes (a = 0) into sendL, side 1 the last column's right nodes
+// (a = P) into sendR; both [field][row][node]. The stage inputs are formed with the same
+// explicitly rounded combinations as the fused kernels' own and halo nodes, so a
+// neighbour's ghost holds the bits its own tile would have formed.
+__global__ void k_pack_ghosts(int mode, const RhsConsts C, const StageArgs A, double* sendL,
+                              double* sendR) {
+  const long long per = (long long)NV * C.Ny * NP;
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 2 * per) return;
+  if (mode != 0 && A.ctrl->done) return;
+  const int side = (int)(q / per);
+  const long long r = q - side * per;
+  const int t = (int)(r % NP), ey = (int)((r / NP) % C.Ny), v = (int)(r / ((long long)NP * C.Ny));
+  const int ex = side == 0 ? 0 : C.Nx - 1, a = side == 0 ? 0 : NP - 1;
+  const long long g = (long long)v * C.Nd + ((long long)ex + (long long)C.Nx * ey) * NPP + a + NP * t;
+  double val;
+  if (mode == 0) {
+    val = A.in[g];
+  } else {
+    const int cur = A.ctrl->cur;
+    const double dt = A.ctrl->dt;
+    if (mode == 1) {
+      const double* k = A.kin_k2 ? A.K2 : A.K1[cur];
+      val = stage_axpy(A.U[cur][g], A.coef * dt, k[g]);
+    } else {
+      val = fsal_finish(A.U[cur][g], fsal_part(A.K1[cur][g], A.K2[g]), A.K3[g], dt);
+    }
+  }
+  (side == 0 ? sendL : sendR)[r] = val;
+}
+
+cudaError_t launch_pack_ghosts(int mode, const RhsConsts& C, const StageArgs& A, double* sendL,
+                               double* sendR, cudaStream_t s) {
+  const long long n = 2LL * NV * C.Ny * NP;
+  const int threads = 256;
+  k_pack_ghosts<<<(unsigned)((n + threads - 1) / threads), threads, 0, s>>>(mode, C, A, sendL,
+                                                                            sendR);
+  return cudaGetLastError();
+}
+
 template <int MODE, int TXs, int TYs>
 static cudaError_t launch_b(int blocks, const BatchArgs& B, cudaStream_t s) {
   const size_t smem = sizeof(typename Tile<TXs, TYs, false>::Smem);

@@ -12,28 +12,37 @@ template <int MODE>
 static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
   const dim3 grid((C.Nx + 7) / 8, (C.Ny + 3) / 4);
   const size_t smem = sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
-  if (C.manning) k_fused<MODE, SGNB_EXACT, true><<<grid, NTHR, smem, s>>>(C, A);
-  else k_fused<MODE, SGNB_EXACT, false><<<grid, NTHR, smem, s>>>(C, A);
+  const bool ghost = C.ghostL != nullptr || C.ghostR != nullptr;
+  if (C.manning) {
+    if (ghost) k_fused<MODE, SGNB_EXACT, true, true><<<grid, NTHR, smem, s>>>(C, A);
+    else k_fused<MODE, SGNB_EXACT, true, false><<<grid, NTHR, smem, s>>>(C, A);
+  } else {
+    if (ghost) k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
+    else k_fused<MODE, SGNB_EXACT, false, false><<<grid, NTHR, smem, s>>>(C, A);
+  }
   return cudaGetLastError();
 }
 
-template <bool FRIC>
-static cudaError_t prepare_fric() {
+template <bool FRIC, bool GHOST>
+static cudaError_t prepare_variant() {
   const int bytes = (int)sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC, GHOST>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC, GHOST>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC>,
+  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC, GHOST>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 static cudaError_t prepare_all() {
-  cudaError_t e = prepare_fric<false>();
-  return e == cudaSuccess ? prepare_fric<true>() : e;
+  cudaError_t e = prepare_variant<false, false>();
+  if (e == cudaSuccess) e = prepare_variant<true, false>();
+  if (e == cudaSuccess) e = prepare_variant<false, true>();
+  if (e == cudaSuccess) e = prepare_variant<true, true>();
+  return e;
 }
 
 static cudaError_t launch_any(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {

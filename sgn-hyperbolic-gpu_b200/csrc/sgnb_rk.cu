@@ -185,6 +185,7 @@ cudaError_t launch_reduce_diag(int what, const RhsConsts& C, const double* U, co
 struct EtaWin {
   double x0, x1, y0, y1, hx, hy;
   double xi[5];
+  int ex0;  // global index of the first element column (slabs)
 };
 
 __global__ void __launch_bounds__(256) k_eta_max(const RhsConsts C, const double* U,
@@ -199,7 +200,7 @@ __global__ void __launch_bounds__(256) k_eta_max(const RhsConsts C, const double
     const long long e = i / 25;
     const int loc = (int)(i - e * 25);
     const int ex = (int)(e % C.Nx), ey = (int)(e / C.Nx);
-    const double x = ex * W.hx + 0.5 * W.hx * (W.xi[loc % 5] + 1.0);
+    const double x = (W.ex0 + ex) * W.hx + 0.5 * W.hx * (W.xi[loc % 5] + 1.0);
     const double y = ey * W.hy + 0.5 * W.hy * (W.xi[loc / 5] + 1.0);
     if (x < W.x0 || x > W.x1 || y < W.y0 || y > W.y1) continue;
     const double eta = U[i] - C.Hnod[i];
@@ -227,10 +228,10 @@ __global__ void __launch_bounds__(256) k_eta_max(const RhsConsts C, const double
 }
 
 cudaError_t launch_eta_max(const RhsConsts& C, const double* U, double x0, double x1, double y0,
-                           double y1, double hx, double hy, const double* xi, double* out,
-                           int nblk, cudaStream_t s) {
+                           double y1, double hx, double hy, int ex0, const double* xi,
+                           double* out, int nblk, cudaStream_t s) {
   EtaWin W;
-  W.x0 = x0; W.x1 = x1; W.y0 = y0; W.y1 = y1; W.hx = hx; W.hy = hy;
+  W.x0 = x0; W.x1 = x1; W.y0 = y0; W.y1 = y1; W.hx = hx; W.hy = hy; W.ex0 = ex0;
   for (int k = 0; k < 5; ++k) W.xi[k] = xi[k];
   k_eta_max<<<nblk, 256, 0, s>>>(C, U, W, out);
   return cudaGetLastError();

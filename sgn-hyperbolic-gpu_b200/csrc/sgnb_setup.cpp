@@ -171,7 +171,7 @@ void node_coords(const Mesh& m, const FrTables& t, double* x, double* y) {
     for (int b = 0; b < np; ++b)
       for (int a = 0; a < np; ++a) {
         const long long g = e * npp + a + np * b;
-        x[g] = ex * m.hx + 0.5 * m.hx * (t.nodes[a] + 1.0);
+        x[g] = (m.ex0 + ex) * m.hx + 0.5 * m.hx * (t.nodes[a] + 1.0);
         y[g] = ey * m.hy + 0.5 * m.hy * (t.nodes[b] + 1.0);
       }
   }
@@ -219,8 +219,8 @@ void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p,
     const int ex = (int)(e % m.Nx), ey = (int)(e / m.Nx);
     for (int s = 0; s < np; ++s) {
       const double yt = ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0);
-      const double xt = ex * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
-      out.HfX[e * np + s] = still_depth(kind, p, ex * m.hx, yt);
+      const double xt = (m.ex0 + ex) * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
+      out.HfX[e * np + s] = still_depth(kind, p, (m.ex0 + ex) * m.hx, yt);
       out.HfY[e * np + s] = still_depth(kind, p, xt, ey * m.hy);
     }
   }
@@ -228,11 +228,12 @@ void bathymetry(const Mesh& m, const FrTables& t, int kind, const double* p,
   for (int ey = 0; ey < m.Ny; ++ey)
     for (int s = 0; s < np; ++s) {
       const double yt = ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0);
-      out.HfXEnd[(size_t)ey * np + s] = still_depth(kind, p, m.Nx * m.hx, yt);
+      out.HfXEnd[(size_t)ey * np + s] =
+          still_depth(kind, p, m.wrapx ? 0.0 : (m.ex0 + m.Nx) * m.hx, yt);
     }
   for (int ex = 0; ex < m.Nx; ++ex)
     for (int s = 0; s < np; ++s) {
-      const double xt = ex * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
+      const double xt = (m.ex0 + ex) * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
       out.HfYEnd[(size_t)ex * np + s] = still_depth(kind, p, xt, m.Ny * m.hy);
     }
 }
@@ -290,17 +291,18 @@ void cells_transpose(const Mesh& m, const FrTables& t, const double* p, const Ba
     const int ex = (int)(e % m.Nx), ey = (int)(e / m.Nx);
     for (int s = 0; s < np; ++s) {
       const double yt = ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0);
-      const double xt = ex * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
-      add(ex * m.hx, yt, bar.HfX[e * np + s]);
+      const double xt = (m.ex0 + ex) * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0);
+      add((m.ex0 + ex) * m.hx, yt, bar.HfX[e * np + s]);
       add(xt, ey * m.hy, bar.HfY[e * np + s]);
     }
   }
   for (int ey = 0; ey < m.Ny; ++ey)
     for (int s = 0; s < np; ++s)
-      add(m.Nx * m.hx, ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0), bar.HfXEnd[(size_t)ey * np + s]);
+      add(m.wrapx ? 0.0 : (m.ex0 + m.Nx) * m.hx, ey * m.hy + 0.5 * m.hy * (t.nodes[s] + 1.0),
+          bar.HfXEnd[(size_t)ey * np + s]);
   for (int ex = 0; ex < m.Nx; ++ex)
     for (int s = 0; s < np; ++s)
-      add(ex * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0), m.Ny * m.hy, bar.HfYEnd[(size_t)ex * np + s]);
+      add((m.ex0 + ex) * m.hx + 0.5 * m.hx * (t.nodes[s] + 1.0), m.Ny * m.hy, bar.HfYEnd[(size_t)ex * np + s]);
 }
 
 }  // namespace sgnb

@@ -15,6 +15,10 @@ struct FrTables {
 struct Mesh {
   int Nx = 0, Ny = 0;
   double Lx = 0, Ly = 0, hx = 0, hy = 0;
+  int ex0 = 0;  // global index of the first element column (slabs of a larger mesh)
+  // the slab's right edge is the periodic wrap of the larger mesh: the depth across it is
+  // sampled at x = 0, where the whole mesh samples the first column's left faces
+  bool wrapx = false;
 };
 
 // Bathymetry statics read by the kernels (SGN2D accessors, src/solver/sgn2d.h:94-98),

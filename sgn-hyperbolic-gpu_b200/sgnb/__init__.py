@@ -66,7 +66,8 @@ class _Desc(C.Structure):
                 ("gRp", _dp), ("qw", _dp),
                 ("bathy_kind", C.c_int), ("bathy_par", _dp), ("n_bathy_par", C.c_int),
                 ("Hnod", _dp), ("Hx", _dp), ("Hy", _dp), ("HfaceX", _dp), ("HfaceY", _dp),
-                ("HfaceXEnd", _dp), ("HfaceYEnd", _dp)]
+                ("HfaceXEnd", _dp), ("HfaceYEnd", _dp),
+                ("Nx_global", C.c_int), ("ex_offset", C.c_int)]
 
 
 class _Opts(C.Structure):
@@ -140,6 +141,15 @@ SIGNATURES = {
                                         C.POINTER(C.c_void_p)]),
     "sgnb_fr_tables": (C.c_int, [C.c_int] + [_dp] * 7),
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
+    "sgnb_set_ghosts": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "sgnb_slab_pack": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_void_p]),
+    "sgnb_slab_begin": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_longlong, _dp,
+                                  C.POINTER(_Opts)]),
+    "sgnb_slab_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "sgnb_slab_partials": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.POINTER(C.c_int)]),
+    "sgnb_slab_control": (C.c_int, [C.c_void_p, _dp, C.c_int, C.c_longlong, C.c_void_p]),
+    "sgnb_slab_status": (C.c_int, [C.c_void_p, C.POINTER(_Stats), C.POINTER(C.c_int),
+                                   C.c_void_p]),
     "sgnb_eta_max": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
                                _dp, C.POINTER(C.c_longlong)]),
     "sgnb_sample_eta": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.c_int, _dp]),
