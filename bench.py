@@ -432,12 +432,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["sgnb", "reference"], default="sgnb")
     ap.add_argument("--precision", choices=["fast", "exact", "mixed"], default="fast")
-    ap.add_argument("--workload", choices=["cfg2", "sweep", "mixed", "adjoint"],
+    ap.add_argument("--workload", choices=["cfg2", "sweep", "mixed", "adjoint", "slabs"],
                     default="cfg2",
                     help="cfg2: the benchmark (default); sweep: the 256-instance batched "
                          "sweep against sequential single-instance runs; mixed: mixed vs "
                          "FP64 on configuration 2 with the eta error; adjoint: "
-                         "configuration 5 forward + VJP")
+                         "configuration 5 forward + VJP; slabs: configuration 2 on x slabs "
+                         "of one device against the whole mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bc", choices=["walls", "periodic"], default="walls",
                     help="boundaries of configuration 2 (periodic: the reference solver's "
@@ -462,6 +463,9 @@ def main():
     elif args.workload == "adjoint":
         from sgnb import benchmarks as BW
         BW.run_adjoint(args, ClockSampler, measured_peak_hbm())
+    elif args.workload == "slabs":
+        from sgnb import benchmarks as BW
+        BW.run_slabs(args, ClockSampler, measured_peak_hbm())
     else:
         run_ours(args)
 

@@ -278,3 +278,86 @@ def run_adjoint(args, clock_sampler, peak):
     A.close()
     d.close()
     print(json.dumps(line), flush=True)
+
+
+def run_slabs(args, clock_sampler, peak):
+    """Configuration 2 on x slabs of one device (1, 2 and 4 slabs: the edge exchange and
+    the partial gather between slabs are device copies on the solver's stream, every
+    stage launched from the host), against the whole-mesh device loop: K accepted steps
+    each from the same state, throughput and the largest relative difference per field
+    of the final states."""
+    import torch
+
+    from .slabs import SlabSolver
+
+    Nx, Ny = W.CFG2["Nx"], W.CFG2["Ny"]
+    if args.mesh:
+        Nx, Ny = args.mesh
+    kw = dict(W.cfg2_solver_args(Nx, Ny), precision=FP64_FAST)
+    dof = 125.0 * Nx * Ny
+    Ud = W.cfg2_state_torch(Nx, Ny)
+
+    def rel(a, b):
+        a, b = a.view(5, -1), b.view(5, -1)
+        out = 0.0
+        for v in range(5):
+            s = float(b[v].abs().max())
+            out = max(out, float((a[v] - b[v]).abs().max()) / (s if s > 0 else 1.0))
+        return out
+
+    with SGN2DB200(**kw) as d:
+        d.upload_tensor(Ud)
+        dt0 = d.cfl_time_step(0.5)
+        d.integrate_steps(0.0, dt0, args.warmup)
+        d.upload_tensor(Ud)
+        _, sp = d.state_device_ptr()
+        stream = torch.cuda.ExternalStream(sp)
+        e0, e1 = _events(torch, stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        st = d.integrate_steps(0.0, dt0, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        whole = dict(value=dof * st.rhsEvals / t, ms_per_step=t / args.steps * 1e3,
+                     accepted=st.accepted, rejected=st.rejected)
+        ref = d.state_tensor().clone()
+    slabs = {}
+    clocks = None
+    for n in (1, 2, 4):
+        with SlabSolver(kw, nslabs=n) as s:
+            s.upload_tensor(Ud)
+            s.integrate_steps(0.0, dt0, args.warmup)
+            s.upload_tensor(Ud)
+            e0, e1 = _events(torch, s.stream)
+            torch.cuda.synchronize()
+            with clock_sampler(0) as clk:
+                e0.record(s.stream)
+                st = s.integrate_steps(0.0, dt0, args.steps)
+                e1.record(s.stream)
+                torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            slabs[str(n)] = dict(value=dof * st.rhsEvals / t, ms_per_step=t / args.steps * 1e3,
+                                 accepted=st.accepted, rejected=st.rejected,
+                                 rel_diff_vs_whole=rel(s.download_tensor(), ref))
+            clocks = clk.summary()
+    top = slabs["4"]
+    edge_bytes = 5 * Ny * 5 * 8
+    line = {
+        "metric": METRIC, "value": top["value"], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": top["ms_per_step"],
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"configuration 2 ({Nx}x{Ny}, walls, adaptive BS3(2)) on 4 x "
+                               "slabs of one device; the whole-mesh loop and 1 and 2 slabs "
+                               "beside it",
+                   "edge_bytes": edge_bytes,
+                   "exchange_bytes_per_attempt_per_slab": 3 * 2 * edge_bytes,
+                   "l2": f"inputs larger than L2 ({8 * 5 * dof / 1e9:.1f} GB per state)"},
+        "whole_mesh": whole, "slabs": slabs,
+        "slab_over_whole": {k: v["value"] / whole["value"] for k, v in slabs.items()},
+        "clocks": clocks, "roofline": None, "gpu_launches": None,
+        "timing": "CUDA events on the solver's stream around the K steps (the host launches "
+                  "every stage and reads the controller every 4 attempts)",
+    }
+    print(json.dumps(line), flush=True)

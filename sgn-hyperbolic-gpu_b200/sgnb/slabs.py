@@ -1,10 +1,11 @@
 """Slab decomposition of one mesh along x: the data-parallel form of the 2D solver.
 
-The reference decomposes its 1D solver into x slabs over MPI (src/parallel/slab1d.h:23-72,
-src/parallel/mpi_slab.cpp:487-537): each rank owns a contiguous run of element columns,
-exchanges the trace nodes across its two slab edges before every right-hand side, and
-takes one global reduction of the error norm per BS3(2) attempt so that every rank makes
-the same accept / reject decision. This module does the same for the 2D hot path:
+The reference's multi-GPU 2D solver splits the mesh into x slabs over MPI
+(src/parallel/slab1d.h:55-72, src/cuda/sgn2d_cuda_mpi.cu:487-537, 605-615): each rank owns
+a contiguous run of element columns, exchanges the traces across its two slab edges before
+every right-hand side (a pack kernel and two MPI_Sendrecv), and takes one global reduction
+of the error norm per BS3(2) attempt so that every rank makes the same accept / reject
+decision. This module does the same for the 2D hot path:
 
 * ``slab_partition`` -- the reference's column split (the first ``Nx % size`` slabs take
   one column more, src/parallel/slab1d.h:55-72), and ``neighbours``.
@@ -261,6 +262,30 @@ class SlabSolver:
         for s in self.slabs:
             s.ctx.upload(self._cols(U, s.ex0, s.nx))
         self.torch.cuda.synchronize(self.device)
+
+    def upload_tensor(self, t):
+        """Device-to-device form of ``upload`` (a float64 tensor of the whole mesh)."""
+        torch = self.torch
+        if t.dtype != torch.float64 or t.numel() != NV * 25 * self.Nx * self.Ny:
+            raise ValueError("SlabSolver.upload_tensor: float64 whole-mesh state expected")
+        v = t.reshape(NV, self.Ny, self.Nx, 25)
+        torch.cuda.synchronize(self.device)
+        for s in self.slabs:
+            s.ctx.state_tensor().view(NV, self.Ny, s.nx, 25).copy_(v[:, :, s.ex0:s.ex0 + s.nx, :])
+        torch.cuda.synchronize(self.device)
+
+    def download_tensor(self):
+        """The whole mesh's state as a new device tensor (single process)."""
+        torch = self.torch
+        if len(self.slabs) != self.size:
+            raise ValueError("SlabSolver.download_tensor: one slab per rank")
+        out = torch.empty((NV, self.Ny, self.Nx, 25), dtype=torch.float64,
+                          device=f"cuda:{self.device}")
+        torch.cuda.synchronize(self.device)
+        for s in self.slabs:
+            out[:, :, s.ex0:s.ex0 + s.nx, :].copy_(s.ctx.state_tensor().view(NV, self.Ny, s.nx, 25))
+        torch.cuda.synchronize(self.device)
+        return out.reshape(-1)
 
     def download_local(self):
         """{slab index: that slab's state} for the local slabs."""

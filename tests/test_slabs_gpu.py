@@ -54,6 +54,10 @@ def test_rhs_bitwise(case, nslabs, bc):
         # upload / download round trip through the column scatter
         s.upload(U)
         assert bits_equal(s.download(), U)
+        import torch
+
+        s.upload_tensor(torch.from_numpy(U[::-1].copy()).cuda())
+        assert bits_equal(s.download_tensor().cpu().numpy(), U[::-1])
 
 
 @pytest.mark.parametrize("bc", [0, 1])
