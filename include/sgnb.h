@@ -216,8 +216,9 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
  *                     `in` of a right-hand side (NULL: the current state), 2 / 3 = the
  *                     intermediate stages of the running attempt, 4 = its end-point
  *                     candidate; sendL / sendR are [5][Ny][5] device arrays
- *   sgnb_slab_begin   the controller for nsteps accepted steps from dt0 (dts != NULL:
- *                     frozen step sizes, the bs3Step replay)
+ *   sgnb_slab_begin   the controller from t0 with dt0 until tEnd (HUGE_VAL: none) or
+ *                     nsteps accepted steps (0: none), whichever comes first (dts != NULL:
+ *                     nsteps frozen step sizes, the bs3Step replay)
  *   sgnb_slab_launch  stage 1 (FSAL head k1 = R(u)), 2, 3, 4 (end point, error partials)
  *   sgnb_slab_partials / sgnb_slab_control / sgnb_slab_status: this slab's partials
  *                     (3 doubles per tile), the controller on the gathered partials of all
@@ -228,8 +229,8 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
 int sgnb_set_ghosts(sgnb_ctx* ctx, const double* ghostL, const double* ghostR);
 int sgnb_slab_pack(sgnb_ctx* ctx, int stage, const double* in, double* sendL, double* sendR,
                    void* stream);
-int sgnb_slab_begin(sgnb_ctx* ctx, double t0, double dt0, long long nsteps, const double* dts,
-                    const sgnb_rk_opts* opts);
+int sgnb_slab_begin(sgnb_ctx* ctx, double t0, double tEnd, double dt0, long long nsteps,
+                    const double* dts, const sgnb_rk_opts* opts);
 int sgnb_slab_launch(sgnb_ctx* ctx, int stage, void* stream);
 int sgnb_slab_partials(sgnb_ctx* ctx, double** partials, int* nblk);
 int sgnb_slab_control(sgnb_ctx* ctx, const double* partials, int nblk, long long n_total,

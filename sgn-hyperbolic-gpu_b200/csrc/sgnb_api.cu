@@ -872,9 +872,10 @@ int sgnb_slab_pack(sgnb_ctx* c, int stage, const double* in, double* sendL, doub
   return SGNB_OK;
 }
 
-int sgnb_slab_begin(sgnb_ctx* c, double t0, double dt0, long long nsteps, const double* dts,
-                    const sgnb_rk_opts* opts) {
-  if (!c || nsteps < 1 || !(dt0 > 0)) return fail(c, SGNB_ERR_INVALID, "nsteps >= 1, dt0 > 0");
+int sgnb_slab_begin(sgnb_ctx* c, double t0, double tEnd, double dt0, long long nsteps,
+                    const double* dts, const sgnb_rk_opts* opts) {
+  if (!c || nsteps < 0 || !(dt0 > 0) || (nsteps == 0 && !(tEnd < 1e300)) || (dts && nsteps < 1))
+    return fail(c, SGNB_ERR_INVALID, "dt0 > 0; nsteps >= 1, or nsteps = 0 and a finite tEnd");
   if (int rc = set_device(c)) return rc;
   sgnb_rk_opts o;
   if (opts) o = *opts; else sgnb_rk_opts_init(&o);
@@ -882,13 +883,16 @@ int sgnb_slab_begin(sgnb_ctx* c, double t0, double dt0, long long nsteps, const 
   init_ctrl(c, h, o);
   h.log = nullptr;
   h.t = t0;
-  h.tEnd = 1e300;
+  h.tEnd = tEnd < 1e300 ? tEnd : 1e300;
   h.dt = (o.dtMax < dt0) ? o.dtMax : dt0;
   h.errPrev = 1.0;
   h.tReached = t0;
   h.cur = c->cur;
   h.rhsEvals = 1;  // the FSAL head
   h.maxAccepted = nsteps;
+  // loop test and end-time clip of the first attempt (rk.cpp:95-97)
+  if (!(h.t < h.tEnd - 1e-15 * ((1.0 < std::fabs(h.tEnd)) ? std::fabs(h.tEnd) : 1.0))) h.done = 1;
+  else if (h.t + h.dt > h.tEnd) h.dt = h.tEnd - h.t;
   if (dts) {  // frozen step sizes (bs3Step replay)
     if (nsteps > c->dtCap) {
       cudaFree(c->dtList);

@@ -143,7 +143,8 @@ SIGNATURES = {
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
     "sgnb_set_ghosts": (C.c_int, [C.c_void_p, _dp, _dp]),
     "sgnb_slab_pack": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_void_p]),
-    "sgnb_slab_begin": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_longlong, _dp,
+    "sgnb_slab_begin": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                  C.c_longlong, _dp,
                                   C.POINTER(_Opts)]),
     "sgnb_slab_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "sgnb_slab_partials": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.POINTER(C.c_int)]),

@@ -14,8 +14,8 @@ decision. This module does the same for the 2D hot path:
 * ``DistExchange`` -- one slab per rank over ``torch.distributed`` (NCCL between GPUs,
   gloo on the host): point-to-point sends of the edge nodes and an all-gather of the
   error partials.
-* ``SlabSolver`` -- ``rhs``, ``integrate_steps`` (adaptive or frozen step sizes),
-  ``upload`` / ``download`` of the whole mesh's state.
+* ``SlabSolver`` -- ``rhs``, ``integrate_adaptive`` (to tEnd), ``integrate_steps``
+  (adaptive or frozen step sizes), ``upload`` / ``download`` of the whole mesh's state.
 
 Each slab is a library context created with ``Nx_global`` / ``ex_offset`` (its node
 coordinates and bathymetry are the whole mesh's), and its two ghost arrays
@@ -330,33 +330,39 @@ class SlabSolver:
         return dU.reshape(-1)
 
     # --- BS3(2) ------------------------------------------------------------------
+    def integrate_adaptive(self, t0, tEnd, dt0, opt: AdaptiveRKOptions | None = None,
+                           check_every: int = 4):
+        """SGN2DCudaMpi::integrateAdaptive (src/cuda/sgn2d_cuda_mpi.h:62): adaptive BS3(2)
+        of the uploaded state from t0 to tEnd."""
+        return self._run(t0, tEnd, dt0, 0, opt, None, check_every, 1 << 40)
+
     def integrate_steps(self, t0, dt0, nsteps, opt: AdaptiveRKOptions | None = None,
                         dts=None, check_every: int = 4):
         """``nsteps`` accepted BS3(2) steps of the uploaded state: adaptive from ``dt0``,
-        or with the frozen step sizes ``dts`` (one per step, every step accepted).
+        or with the frozen step sizes ``dts`` (one per step, every step accepted)."""
+        if dts is not None and np.asarray(dts).size != nsteps:
+            raise ValueError("integrate_steps: one frozen step size per step")
+        return self._run(t0, float("inf"), dt0, nsteps, opt, dts, check_every,
+                         64 * int(nsteps) + 4096)
 
-        Per attempt: stages 2, 3, 4, each after an edge exchange of its stage inputs, then
-        the gather of all slabs' error partials and every slab's controller on them. The
-        host reads the controller every ``check_every`` attempts (the kernels of attempts
-        after the end return at once)."""
+    def _run(self, t0, tEnd, dt0, nsteps, opt, dts, check_every, limit):
+        """Per attempt: stages 2, 3, 4, each after an edge exchange of its stage inputs,
+        then the gather of all slabs' error partials and every slab's controller on them.
+        The host reads the controller every ``check_every`` attempts (the kernels of
+        attempts after the end return at once); ``limit`` bounds the attempts."""
         torch = self.torch
         sp = self.stream.cuda_stream
         o = _Opts(**dataclasses.asdict(opt or AdaptiveRKOptions()))
-        d = None
-        if dts is not None:
-            d = np.ascontiguousarray(dts, dtype=np.float64)
-            if d.size != nsteps:
-                raise ValueError("integrate_steps: one frozen step size per step")
+        d = None if dts is None else np.ascontiguousarray(dts, dtype=np.float64)
         torch.cuda.synchronize(self.device)
         for s in self.slabs:
-            _check(lib().sgnb_slab_begin(s.h, float(t0), float(dt0), int(nsteps),
+            _check(lib().sgnb_slab_begin(s.h, float(t0), float(tEnd), float(dt0), int(nsteps),
                                          None if d is None else d.ctypes.data_as(_dp),
                                          C.byref(o)), s.h)
         # FSAL head: k1 = R(u)
         self._exchange(0)
         for s in self.slabs:
             _check(lib().sgnb_slab_launch(s.h, 1, C.c_void_p(sp)), s.h)
-        limit = 64 * int(nsteps) + 4096  # attempts; a run that ends stops the loop earlier
         attempts = 0
         done = C.c_int(0)
         st = _Stats()

@@ -122,3 +122,26 @@ def test_slab_contexts_refuse_whole_mesh_entries():
             SGNAdjoint(ctx, [1e-3], [0])
     with pytest.raises(sgnb.SgnbError):
         SlabSolver(dict(kw, precision=sgnb.MIXED), nslabs=2)
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_adaptive_to_end_time(bc):
+    """integrateAdaptive to tEnd: the same attempts and end time as the whole mesh."""
+    kw, U = shoal_case(bc, Nx=13, Ny=5)
+    kw = dict(kw, precision=sgnb.FP64_FAST)
+    with sgnb.SGN2DB200(**kw) as d:
+        d.upload(U)
+        dt0 = d.cfl_time_step(0.5)
+        tEnd = 7.3 * dt0
+        st1 = d.integrate_adaptive(0.0, tEnd, dt0)
+        ref = d.download()
+    with SlabSolver(kw, nslabs=3) as s:
+        s.upload(U)
+        st = s.integrate_adaptive(0.0, tEnd, dt0)
+        assert (st.accepted, st.rejected, st.rhsEvals) == (st1.accepted, st1.rejected,
+                                                           st1.rhsEvals)
+        assert abs(st.tReached - tEnd) <= 1e-14 * tEnd and abs(st1.tReached - tEnd) <= 1e-14 * tEnd
+        assert rel_per_field(s.download(), ref) < 1e-10
+        # a run that starts at its end time takes no step
+        st0 = s.integrate_adaptive(tEnd, tEnd, dt0)
+        assert st0.accepted == 0 and st0.rejected == 0
