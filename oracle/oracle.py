@@ -28,6 +28,8 @@ LIB_REFERENCE = os.path.join(HERE, "_ref", "libsgnref.so")
 
 BC_PERIODIC = 0
 BC_WALL = 1
+POINTS_GLL = 0    # solution points (PointSet, src/core/fr_operators.h:51)
+POINTS_GAUSS = 1
 
 BATHY_NONE = 0
 BATHY_CONST = 1
@@ -79,6 +81,8 @@ def _load(path: str) -> C.CDLL:
     lib.or_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                               C.c_double, C.c_double, C.c_double, C.c_double,
                               C.c_int, C.c_int, C.c_int, _dp, C.c_int]
+    lib.or_create_points.restype = C.c_void_p
+    lib.or_create_points.argtypes = lib.or_create.argtypes + [C.c_int]
     lib.or_destroy.argtypes = [C.c_void_p]
     lib.or_ndof.restype = C.c_long
     lib.or_ndof.argtypes = [C.c_void_p]
@@ -120,7 +124,7 @@ class Oracle:
 
     def __init__(self, P=4, Nx=8, Ny=6, Lx=10.0, Ly=8.0, g=9.81, c=0.0, gamma=1.5,
                  nManning=0.0, bc_x=BC_PERIODIC, bc_y=BC_PERIODIC, bathy_kind=BATHY_NONE,
-                 bathy_par=(), reference=False):
+                 bathy_par=(), reference=False, points=POINTS_GLL):
         self.lib = _load(LIB_REFERENCE if reference else LIB_RESTATEMENT)
         self.P, self.Nx, self.Ny, self.Lx, self.Ly = P, Nx, Ny, Lx, Ly
         self.np_ = P + 1
@@ -128,8 +132,10 @@ class Oracle:
         self._bp = np.ascontiguousarray(np.asarray(bathy_par, dtype=np.float64).reshape(-1))
         if self._bp.size == 0:
             self._bp = np.zeros(1)
-        self.h = self.lib.or_create(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y,
-                                    bathy_kind, _ptr(self._bp), int(self._bp.size))
+        self.points = points
+        self.h = self.lib.or_create_points(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x,
+                                           bc_y, bathy_kind, _ptr(self._bp),
+                                           int(self._bp.size), points)
         if not self.h:
             raise ValueError("invalid solver arguments")
         self.Nd = int(self.lib.or_ndof(self.h))

@@ -10,7 +10,9 @@
 // reference itself: the state is mirror-copied onto the doubled domain
 // [0,2Lx] x [0,2Ly] (normal momentum negated in the mirror images), the periodic
 // reference rhs runs there, and the first quadrant is returned. With GLL points the
-// face traces are node values, so this is exactly the mirror-ghost wall.
+// face traces are node values, so this is exactly the mirror-ghost wall. With Gauss
+// points the mirror element's trace is interpolated with lR where the restatement
+// mirrors the own trace formed with lL: equal to round-off, not bit for bit.
 #include "sgn_oracle.h"
 #include "or_bathy.h"
 
@@ -92,6 +94,13 @@ extern "C" {
 or_ctx* or_create(int P, int Nx, int Ny, double Lx, double Ly, double g, double c,
                   double gamma, double nManning, int bc_x, int bc_y, int bathy_kind,
                   const double* bp, int n_par) {
+  return or_create_points(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y, bathy_kind,
+                          bp, n_par, OR_POINTS_GLL);
+}
+
+or_ctx* or_create_points(int P, int Nx, int Ny, double Lx, double Ly, double g, double c,
+                         double gamma, double nManning, int bc_x, int bc_y, int bathy_kind,
+                         const double* bp, int n_par, int points) {
   try {
     auto* s = new or_ctx();
     s->Nx = Nx; s->Ny = Ny; s->np = P + 1; s->npp = (P + 1) * (P + 1);
@@ -109,7 +118,9 @@ or_ctx* or_create(int P, int Nx, int Ny, double Lx, double Ly, double g, double 
       const std::vector<double>* pv = &s->bpar;
       depth = [kind, pv](double x, double y) { return or_bathy_eval(kind, pv->data(), x, y); };
     }
-    s->sys.reset(new sgn::SGN2D(P, s->Nx2, s->Ny2, Lx2, Ly2, par, depth));
+    const sgn::PointSet ps =
+        points == OR_POINTS_GAUSS ? sgn::PointSet::GaussLegendre : sgn::PointSet::GaussLobatto;
+    s->sys.reset(new sgn::SGN2D(P, s->Nx2, s->Ny2, Lx2, Ly2, par, depth, ps));
     return s;
   } catch (...) {
     return nullptr;

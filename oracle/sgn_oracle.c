@@ -29,6 +29,7 @@ enum { NVAR = 5, IH = 0, IHU = 1, IHV = 2, IHW = 3, IHP = 4 };
 
 struct or_ctx {
   int P, np, npp, Nx, Ny, ne;
+  int points;  /* OR_POINTS_GLL or OR_POINTS_GAUSS (PointSet, fr_operators.h) */
   long Nd;
   double Lx, Ly, hx, hy, Jx, Jy;
   double g, c, gamma, nManning;
@@ -85,6 +86,24 @@ static void gll_nodes(int P, double* x) {
   }
 }
 
+/* Gauss-Legendre nodes: the P+1 roots of L_{P+1} by Newton's method from the
+ * asymptotic guesses -cos(pi (i + 3/4) / (n + 1/2)) (fr_operators.cpp:86-100). */
+static void gauss_nodes(int P, double* x) {
+  const double kPi = 3.14159265358979323846;
+  const int n = P + 1;
+  for (int i = 0; i < n; ++i) {
+    double xi = -cos(kPi * (i + 0.75) / (n + 0.5));
+    for (int it = 0; it < 100; ++it) {
+      const double f = leg(n, xi);
+      const double fp = legd(n, xi);
+      const double dx = f / fp;
+      xi -= dx;
+      if (fabs(dx) < 1e-15) break;
+    }
+    x[i] = xi;
+  }
+}
+
 /* Lagrange basis j at xq, barycentric form, exact Kronecker delta on a node
  * (fr_operators.cpp:118-127). */
 static double lagrange_at(int n, const double* x, const double* w, int j, double xq) {
@@ -96,10 +115,11 @@ static double lagrange_at(int n, const double* x, const double* w, int j, double
   return num / den;
 }
 
-/* FROperators1D constructor, GLL branch (fr_operators.cpp:134-200). */
+/* FROperators1D constructor (fr_operators.cpp:134-200). */
 static void build_tables(or_ctx* s) {
   const int P = s->P, n = P + 1;
-  gll_nodes(P, s->xi);
+  if (s->points == OR_POINTS_GAUSS) gauss_nodes(P, s->xi);
+  else gll_nodes(P, s->xi);
   /* barycentric weights (fr_operators.cpp:103-113) */
   for (int j = 0; j < n; ++j) {
     double prod = 1.0;
@@ -131,9 +151,14 @@ static void build_tables(or_ctx* s) {
     s->gLp[i] = 0.5 * signP * (dLP - dLP1);
     s->gRp[i] = 0.5 * (dLP + dLP1);
   }
-  /* GLL quadrature weights (:183-199) */
+  /* quadrature weights (:183-199) */
   if (P == 0) {
     s->qw[0] = 2.0;
+  } else if (s->points == OR_POINTS_GAUSS) {
+    for (int i = 0; i < n; ++i) {
+      const double dLP1 = legd(P + 1, s->xi[i]);
+      s->qw[i] = 2.0 / ((1.0 - s->xi[i] * s->xi[i]) * dLP1 * dLP1);
+    }
   } else {
     for (int i = 0; i < n; ++i) {
       const double LP = leg(P, s->xi[i]);
@@ -254,9 +279,20 @@ void or_node_coords(const or_ctx* s, double* x, double* y) {
 or_ctx* or_create(int P, int Nx, int Ny, double Lx, double Ly, double g, double c,
                   double gamma, double nManning, int bc_x, int bc_y, int bathy_kind,
                   const double* bp, int n_par) {
+  return or_create_points(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y, bathy_kind,
+                          bp, n_par, OR_POINTS_GLL);
+}
+
+or_ctx* or_create_points(int P, int Nx, int Ny, double Lx, double Ly, double g, double c,
+                         double gamma, double nManning, int bc_x, int bc_y, int bathy_kind,
+                         const double* bp, int n_par, int points) {
   (void)n_par;
   if (P < 1 || Nx < 2 || Ny < 2) return NULL; /* sgn2d.cpp:36 */
+  if (points != OR_POINTS_GLL && points != OR_POINTS_GAUSS) return NULL;
+  /* bathymetry requires GLL points (sgn2d.cpp:46-47) */
+  if (points != OR_POINTS_GLL && bathy_kind != OR_BATHY_NONE) return NULL;
   or_ctx* s = (or_ctx*)calloc(1, sizeof(or_ctx));
+  s->points = points;
   s->P = P; s->np = P + 1; s->npp = (P + 1) * (P + 1);
   s->Nx = Nx; s->Ny = Ny; s->ne = Nx * Ny;
   s->Nd = (long)s->ne * s->npp;
@@ -385,14 +421,14 @@ void or_set_bathymetry(or_ctx* s, const double* Hnod, const double* Hx, const do
 /* rhs: src/solver/sgn2d.cpp:125-290                                          */
 /* ------------------------------------------------------------------------- */
 
-/* [not in the reference] mirror ghost of a face state across a wall normal to
- * direction dir: the normal momentum changes sign. Written as the trace of the
- * mirrored node value (0.0 + (-v)), which is what the periodic reference computes
- * for the mirror-image element of the doubled domain. */
-static void mirror_ghost(const double* own_node, int dir, double* ghost) {
-  for (int v = 0; v < NVAR; ++v) ghost[v] = 0.0 + own_node[v];
+/* [not in the reference] mirror ghost of the element's own face trace across a wall
+ * normal to direction dir: the normal momentum changes sign, written 0.0 + (-v). With
+ * GLL points the trace is 0.0 + the edge node, and this is what the periodic reference
+ * computes for the mirror-image element of the doubled domain. */
+static void mirror_ghost(const double* own_trace, int dir, double* ghost) {
+  for (int v = 0; v < NVAR; ++v) ghost[v] = 0.0 + own_trace[v];
   const int n = (dir == 0) ? IHU : IHV;
-  ghost[n] = 0.0 + (-own_node[n]);
+  ghost[n] = 0.0 + (-own_trace[n]);
 }
 
 int or_rhs(const or_ctx* s, const double* U, double* dU) {
@@ -462,19 +498,17 @@ int or_rhs(const or_ctx* s, const double* U, double* dU) {
 
     /* 3) Rusanov fluxes and central depths on the four face lines (:198-227) */
     for (int b = 0; b < np; ++b) {
-      double gL[NVAR], gR[NVAR], nodeL[NVAR], nodeR[NVAR];
+      double gL[NVAR], gR[NVAR];
       const double* uL = &xFaceR[((size_t)eL * np + b) * NVAR];
       const double* uMe = &xFaceL[((size_t)e * np + b) * NVAR];
       const double* uR = &xFaceL[((size_t)eR * np + b) * NVAR];
       const double* uMeR = &xFaceR[((size_t)e * np + b) * NVAR];
       if (wallL) {
-        for (int v = 0; v < NVAR; ++v) nodeL[v] = U[UIDX(e, 0, b, v)];
-        mirror_ghost(nodeL, 0, gL);
+        mirror_ghost(uMe, 0, gL);
         uL = gL;
       }
       if (wallR) {
-        for (int v = 0; v < NVAR; ++v) nodeR[v] = U[UIDX(e, np - 1, b, v)];
-        mirror_ghost(nodeR, 0, gR);
+        mirror_ghost(uMeR, 0, gR);
         uR = gR;
       }
       const double HxL = s->HfaceX[e * np + b];
@@ -485,19 +519,17 @@ int or_rhs(const or_ctx* s, const double* U, double* dU) {
       hSxR[b] = 0.5 * (uMeR[IH] + uR[IH]);
     }
     for (int a = 0; a < np; ++a) {
-      double gB[NVAR], gT[NVAR], nodeB[NVAR], nodeT[NVAR];
+      double gB[NVAR], gT[NVAR];
       const double* uB = &yFaceT[((size_t)eB * np + a) * NVAR];
       const double* uMe = &yFaceB[((size_t)e * np + a) * NVAR];
       const double* uT = &yFaceB[((size_t)eT * np + a) * NVAR];
       const double* uMeT = &yFaceT[((size_t)e * np + a) * NVAR];
       if (wallB) {
-        for (int v = 0; v < NVAR; ++v) nodeB[v] = U[UIDX(e, a, 0, v)];
-        mirror_ghost(nodeB, 1, gB);
+        mirror_ghost(uMe, 1, gB);
         uB = gB;
       }
       if (wallT) {
-        for (int v = 0; v < NVAR; ++v) nodeT[v] = U[UIDX(e, a, np - 1, v)];
-        mirror_ghost(nodeT, 1, gT);
+        mirror_ghost(uMeT, 1, gT);
         uT = gT;
       }
       const double HyB = s->HfaceY[e * np + a];

@@ -31,6 +31,8 @@ extern "C" {
 #endif
 
 enum { OR_BC_PERIODIC = 0, OR_BC_WALL = 1 };
+/* solution points (PointSet, src/core/fr_operators.h) */
+enum { OR_POINTS_GLL = 0, OR_POINTS_GAUSS = 1 };
 
 typedef struct or_ctx or_ctx;
 
@@ -39,6 +41,12 @@ typedef struct or_ctx or_ctx;
 or_ctx* or_create(int P, int Nx, int Ny, double Lx, double Ly, double g, double c,
                   double gamma, double nManning, int bc_x, int bc_y, int bathy_kind,
                   const double* bathy_par, int n_par);
+/* The same with the solution point set: Gauss points need a flat bottom (bathy_kind
+ * OR_BATHY_NONE, H = 0), as SGN2D requires (sgn2d.cpp:46-47); their face traces are
+ * interpolated with lL / lR, and a wall mirrors the element's own face trace. */
+or_ctx* or_create_points(int P, int Nx, int Ny, double Lx, double Ly, double g, double c,
+                         double gamma, double nManning, int bc_x, int bc_y, int bathy_kind,
+                         const double* bathy_par, int n_par, int points);
 void or_destroy(or_ctx* s);
 long or_ndof(const or_ctx* s); /* nodes per field, SGN2D::nDof */
 

@@ -8,6 +8,8 @@ state's own round-off is irrelevant to parity.
 Cases:
   bump_case     the GPU parity case of the reference (test/test_cuda_sgn2d.cu:38-64)
   lake_case     lake at rest over the same bump (test/test_sgn2d.cpp:55-66)
+  gauss_case    Gauss-Legendre solution points (PointSet::GaussLegendre): flat bottom
+                H = 0, which SGN2D requires for them (sgn2d.cpp:46-47), smooth state
   cfg1_case     configuration 1: 128x64 on 20x10, flat depth 1, Gaussian hump of 0.05
   cfg2_case     configuration 2: 2048x1024 on 40x20 with reflective walls, 0.45 plane with
                 an elliptic shoal (semi-axes 4 x 3, crest depth 0.15, centred), and 8
@@ -45,6 +47,25 @@ def gll5():
     """GLL nodes for P = 4 (closed form: 0, +-sqrt(3/7), +-1)."""
     s = np.sqrt(3.0 / 7.0)
     return np.array([-1.0, -s, 0.0, s, 1.0])
+
+
+def gauss5():
+    """Gauss-Legendre nodes for P = 4 (the roots of L_5, closed form)."""
+    r = np.sqrt(5.0 - 2.0 * np.sqrt(10.0 / 7.0)) / 3.0
+    s = np.sqrt(5.0 + 2.0 * np.sqrt(10.0 / 7.0)) / 3.0
+    return np.array([-s, -r, 0.0, r, s])
+
+
+def gauss_case(bc=BC_PERIODIC, Nx=8, Ny=6, Lx=10.0, Ly=8.0):
+    c = ALPHA * np.sqrt(G * 1.0)
+    kw = dict(P=4, Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, g=G, c=c, gamma=GAMMA, bc_x=bc, bc_y=bc,
+              bathy_kind=BATHY_NONE, bathy_par=(), points=1)
+    x, y = node_coords(4, Nx, Ny, Lx, Ly, gauss5())
+    kx, ky = 2 * np.pi / Lx, 2 * np.pi / Ly
+    U = make_state(1.0 + 0.04 * np.sin(kx * x) * np.cos(ky * y) + 0.01 * np.cos(2 * kx * x),
+                   0.08 * np.cos(kx * x) * (1 - bc), -0.05 * np.sin(ky * y) * (1 - bc),
+                   0.02 * np.sin(kx * x), 0.01 * np.cos(ky * y))
+    return kw, U
 
 
 def make_state(h, u, v, w, p):

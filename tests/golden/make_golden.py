@@ -15,6 +15,8 @@ Fixtures (golden.npz):
                 rhs bytes, 64 sampled entries, the adaptive run to 100 accepted steps
                 (stats, the accepted step sizes, sha256 + samples of the final state)
   run_*         a short adaptive run of the bump case (tEnd 0.05, atol 1e-10, rtol 1e-8)
+  gauss_*       Gauss-Legendre points (tests/cases.py gauss_case, flat bottom H = 0): the
+                FR tables, the state and its rhs, periodic; the same short adaptive run
 """
 from __future__ import annotations
 
@@ -31,7 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
 sys.path.insert(0, os.path.dirname(HERE))
-from cases import bump_case, cfg1_case, CFG1_STEPS  # noqa: E402
+from cases import bump_case, cfg1_case, gauss_case, CFG1_STEPS  # noqa: E402
 
 
 def sha(a: np.ndarray) -> str:
@@ -63,6 +65,18 @@ def main() -> None:
     out["run_dt0"] = np.array([dt0])
     out["run_stats"] = np.array([st["accepted"], st["rejected"], st["rhsEvals"]], dtype=np.int64)
     out["run_U"] = u
+    # --- Gauss-Legendre points ------------------------------------------------------------
+    kw, U = gauss_case()
+    ref = O.Oracle(reference=True, **kw)
+    for k, a in ref.tables().items():
+        out[f"gauss_{k}"] = a
+    out["gauss_U"] = U
+    out["gauss_R"] = ref.rhs(U)
+    dt0 = ref.cfl_time_step(U, 0.5)
+    u, st, _ = ref.integrate_adaptive(U, 0.0, 0.05, dt0, atol=1e-10, rtol=1e-8)
+    out["gauss_run_stats"] = np.array([st["accepted"], st["rejected"], st["rhsEvals"]],
+                                      dtype=np.int64)
+    out["gauss_run_U"] = u
     # --- configuration 1 -----------------------------------------------------------------
     kw, U = cfg1_case()
     ref = O.Oracle(reference=True, **kw)

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from cases import bump_case, cfg1_case, CFG1_STEPS, lake_case
+from cases import bump_case, cfg1_case, gauss_case, CFG1_STEPS, lake_case
 from conftest import bits_equal
 
 
@@ -127,6 +127,48 @@ def test_cfg1_vs_golden(golden):
     assert [st["accepted"], st["rejected"], st["rhsEvals"]] == list(golden["cfg1_stats"])
     assert hashlib.sha256(u.tobytes()).hexdigest() == str(golden["cfg1_final_sha"][0])
     assert o.mass(U) == golden["cfg1_mass"][0] and o.mass(u) == golden["cfg1_mass"][1]
+
+
+# --------------------------------------------------------------------------- Gauss points
+def test_gauss_vs_golden(golden):
+    """Gauss-Legendre points: FR tables, rhs and a short adaptive run of the reference."""
+    kw, U = gauss_case()
+    o = oracle_for(kw)
+    for k, a in o.tables().items():
+        assert bits_equal(a, golden[f"gauss_{k}"]), k
+    assert bits_equal(U, golden["gauss_U"])
+    assert bits_equal(o.rhs(U), golden["gauss_R"])
+    u, st, _ = o.integrate_adaptive(U, 0.0, 0.05, o.cfl_time_step(U, 0.5), atol=1e-10,
+                                    rtol=1e-8)
+    assert [st["accepted"], st["rejected"], st["rhsEvals"]] == list(golden["gauss_run_stats"])
+    assert bits_equal(u, golden["gauss_run_U"])
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_gauss_vs_reference(need_reference, bc):
+    """Periodic: bit for bit. Walls: the restatement mirrors the own trace, the reference
+    (on the mirror-doubled domain) interpolates the mirror element's trace with lR, which
+    equals lL reversed to round-off only."""
+    kw, U = gauss_case(bc, Nx=7, Ny=5)
+    R, Rref = oracle_for(kw).rhs(U), oracle_for(kw, reference=True).rhs(U)
+    if bc == 0:
+        assert bits_equal(R, Rref)
+    else:
+        # round-off of the face traces (O(1) fluxes); the h field's own rhs is small here
+        assert np.abs(R - Rref).max() <= 1e-13 * np.abs(Rref).max()
+        assert not np.array_equal(R, oracle_for(dict(kw, bc_x=0, bc_y=0)).rhs(U))
+
+
+def test_gauss_needs_flat_bottom_and_keeps_freestream():
+    kw, _ = gauss_case()
+    with pytest.raises(ValueError):
+        oracle_for(dict(kw, bathy_kind=O.BATHY_GAUSS, bathy_par=(1.0, 0.4, 5.0, 4.0, 6.0)))
+    o = oracle_for(kw)
+    n = o.Nd
+    U = o.make_state(np.full(n, 1.0), np.full(n, 0.5), np.full(n, -0.3), np.zeros(n), np.zeros(n))
+    assert np.abs(o.rhs(U)).max() < 1e-11
+    # Gauss quadrature integrates the constant depth exactly: mass = h Lx Ly
+    assert abs(o.mass(U) - 80.0) < 1e-12
 
 
 # --------------------------------------------------------------------------- known answers
