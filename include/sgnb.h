@@ -9,7 +9,8 @@
  *
  * State layout (unchanged from the reference, src/solver/sgn2d.h:22-27):
  * variable-major doubles U[v * Nd + e * 25 + a + 5 b], v in (h, hu, hv, hw, hp),
- * element e = ex + Nx ey, node (a, b) of the 5 x 5 GLL grid, Nd = 25 Nx Ny.
+ * element e = ex + Nx ey, node (a, b) of the 5 x 5 grid of solution points (GLL, or
+ * Gauss-Legendre with point_set), Nd = 25 Nx Ny.
  *
  * Errors: every function returns an sgnb_status; nothing aborts the process
  * (the reference aborts on CUDA errors, src/cuda/sgn2d_cuda.cu:29-37).
@@ -37,6 +38,11 @@ typedef enum {
 } sgnb_status;
 
 enum { SGNB_BC_PERIODIC = 0, SGNB_BC_WALL = 1 };
+
+/* Solution points (PointSet, src/core/fr_operators.h:51). Gauss-Legendre points need a
+ * flat bottom (SGNB_BATHY_NONE: H = 0), as SGN2D requires (sgn2d.cpp:46-47); their face
+ * traces are interpolated with lL / lR, and a wall mirrors the element's own trace. */
+enum { SGNB_POINTS_GLL = 0, SGNB_POINTS_GAUSS = 1 };
 
 /* Arithmetic modes. */
 enum {
@@ -85,6 +91,10 @@ typedef struct {
    * this context owns the Nx columns from ex_offset on; node coordinates, bathymetry and
    * face depths are the full mesh's. Nx_global = 0: the context is the whole mesh. */
   int Nx_global, ex_offset;
+  /* SGNB_POINTS_*, the PointSet argument of SGN2D (sgn2d.h:57-59); caller-given tables
+   * whose lL / lR are not unit rows are Gauss points whatever this says. Gauss points
+   * run in the FP64 modes on whole meshes (not batched, no adjoint). */
+  int point_set;
 } sgnb_desc;
 
 /* AdaptiveRKOptions (src/solver/rk.h:53-61). */
@@ -197,6 +207,9 @@ int sgnb_state_device_ptr(sgnb_ctx* ctx, double** U_dev, void** stream);
  * the host without a device. Sizes P+1, (P+1)^2 for D. */
 int sgnb_fr_tables(int P, double* nodes, double* D, double* lL, double* lR, double* gLp,
                    double* gRp, double* qw);
+/* The same for a point set (SGNB_POINTS_*): FROperators1D(P, pointSet). */
+int sgnb_fr_tables_points(int P, int point_set, double* nodes, double* D, double* lL,
+                          double* lR, double* gLp, double* gRp, double* qw);
 /* The bathymetry arrays sgnb_create would upload for d (SGN2D ctor,
  * src/solver/sgn2d.cpp:30-84), on the host without a device. Any pointer may be NULL. */
 int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* Hy,

@@ -178,6 +178,7 @@ int sgnb_adj_create(sgnb_ctx* c, long long nsteps, const double* dts, int ngauge
   if (c->mixed) return afail(c, SGNB_ERR_UNSUPPORTED, "the adjoint runs in FP64 modes");
   if (c->desc.Nx_global > 0 || c->C.ghostL || c->C.ghostR)
     return afail(c, SGNB_ERR_UNSUPPORTED, "the adjoint runs on whole meshes");
+  if (c->tab.gauss) return afail(c, SGNB_ERR_UNSUPPORTED, "the adjoint runs on GLL points");
   for (int g = 0; g < ngauges; ++g)
     if (gauge_nodes[g] < 0 || gauge_nodes[g] >= c->Nd)
       return afail(c, SGNB_ERR_INVALID, "gauge node out of range");

@@ -108,6 +108,8 @@ int check_desc(const sgnb_desc* d) {
     return fail(nullptr, SGNB_ERR_INVALID, "slab: 0 <= ex_offset, ex_offset + Nx <= Nx_global");
   if ((long long)d->Nx * d->Ny > (1ll << 31) / 25)
     return fail(nullptr, SGNB_ERR_INVALID, "mesh too large");
+  if (d->point_set != SGNB_POINTS_GLL && d->point_set != SGNB_POINTS_GAUSS)
+    return fail(nullptr, SGNB_ERR_INVALID, "point_set must be SGNB_POINTS_GLL or SGNB_POINTS_GAUSS");
   if (d->bathy_kind == SGNB_BATHY_ARRAYS) {
     if (!d->Hnod || !d->Hx || !d->Hy || !d->HfaceX || !d->HfaceY)
       return fail(nullptr, SGNB_ERR_INVALID, "SGNB_BATHY_ARRAYS needs Hnod, Hx, Hy, HfaceX, HfaceY");
@@ -124,7 +126,7 @@ int check_desc(const sgnb_desc* d) {
 
 // FR tables: the caller's (copied from a reference FROperators1D) or built here.
 int tables_for(const sgnb_desc* d, FrTables& t) {
-  fr_tables(d->P, t);
+  fr_tables(d->P, t, d->point_set == SGNB_POINTS_GAUSS);
   const int n = d->P + 1;
   if (d->nodes) std::memcpy(t.nodes, d->nodes, n * sizeof(double));
   if (d->D) std::memcpy(t.D, d->D, n * n * sizeof(double));
@@ -133,10 +135,31 @@ int tables_for(const sgnb_desc* d, FrTables& t) {
   if (d->gLp) std::memcpy(t.gLp, d->gLp, n * sizeof(double));
   if (d->gRp) std::memcpy(t.gRp, d->gRp, n * sizeof(double));
   if (d->qw) std::memcpy(t.qw, d->qw, n * sizeof(double));
-  // the kernels read face traces as the edge nodes: require GLL unit rows
-  for (int j = 0; j < n; ++j) {
-    if (t.lL[j] != (j == 0 ? 1.0 : 0.0) || t.lR[j] != (j == n - 1 ? 1.0 : 0.0))
-      return fail(nullptr, SGNB_ERR_UNSUPPORTED, "only Gauss-Lobatto points are built");
+  // unit face rows: the traces are the edge nodes (GLL); otherwise the Gauss-point kernels
+  // interpolate them
+  bool unit = true;
+  for (int j = 0; j < n; ++j)
+    unit = unit && t.lL[j] == (j == 0 ? 1.0 : 0.0) && t.lR[j] == (j == n - 1 ? 1.0 : 0.0);
+  t.gauss = !unit;
+  if (t.gauss) {
+    // a flat bottom H = 0 (sgn2d.cpp:46-47): no profile, or arrays that are all zero (the
+    // accessors of a reference SGN2D built with Gauss points)
+    bool flat = d->bathy_kind == SGNB_BATHY_NONE;
+    if (d->bathy_kind == SGNB_BATHY_ARRAYS) {
+      const long long ne = (long long)d->Nx * d->Ny, Nd = 25 * ne;
+      auto zero = [](const double* a, long long m) {
+        for (long long i = 0; a && i < m; ++i)
+          if (a[i] != 0.0) return false;
+        return true;
+      };
+      flat = zero(d->Hnod, Nd) && zero(d->Hx, Nd) && zero(d->Hy, Nd) && zero(d->HfaceX, 5 * ne) &&
+             zero(d->HfaceY, 5 * ne) && zero(d->HfaceXEnd, 5 * d->Ny) && zero(d->HfaceYEnd, 5 * d->Nx);
+    }
+    if (!flat) return fail(nullptr, SGNB_ERR_INVALID, "SGN2D: bathymetry requires GLL points");
+    if (d->precision == SGNB_MIXED)
+      return fail(nullptr, SGNB_ERR_UNSUPPORTED, "Gauss points run in the FP64 modes");
+    if (d->Nx_global > 0)
+      return fail(nullptr, SGNB_ERR_UNSUPPORTED, "Gauss points run on whole meshes");
   }
   return SGNB_OK;
 }
@@ -172,7 +195,11 @@ void fill_consts(sgnb_ctx* c) {
   for (int k = 0; k < 5; ++k) {
     C.gLp[k] = c->tab.gLp[k];
     C.gRp[k] = c->tab.gRp[k];
+    C.lL[k] = c->tab.lL[k];
+    C.lR[k] = c->tab.lR[k];
   }
+  C.gauss = c->tab.gauss;
+  C.tr = c->trbuf;
 }
 
 int build_chunk_graph(sgnb_ctx* c, int len) {
@@ -209,8 +236,9 @@ int run_loop(sgnb_ctx* c) {
   int rc = build_chunk_graph(c, len);
   if (rc) return rc;
   SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
-  c->launches = 1 + 4LL * len;  // head + the first chunk
-  // FSAL head: k1 = R(u)
+  // kernels per right-hand side: the fused kernel, after the trace pre-pass for Gauss points
+  const long long per_rhs = c->tab.gauss ? 2 : 1, per_attempt = 3 * per_rhs + 1;
+  c->launches = per_rhs + per_attempt * len;  // head + the first chunk
   // FSAL head: k1 = R(u) into K1[cur] (FP32 in the mixed mode)
   SGNB_CU(c, launch(c, rhs_launch(c->U[c->cur], c->mixed ? nullptr : (double*)c->K1[c->cur]),
                     c->stream));
@@ -220,7 +248,7 @@ int run_loop(sgnb_ctx* c) {
   SGNB_CU(c, cudaEventRecord(c->evRead, c->stream));
   for (long long guard = 0;; ++guard) {
     SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
-    c->launches += 4LL * len;
+    c->launches += per_attempt * len;
     SGNB_CU(c, cudaEventSynchronize(c->evRead));
     if (c->hctrl->done) break;
     SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
@@ -279,6 +307,24 @@ int sgnb_fr_tables(int P, double* nodes, double* D, double* lL, double* lR, doub
   return SGNB_OK;
 }
 
+int sgnb_fr_tables_points(int P, int point_set, double* nodes, double* D, double* lL,
+                          double* lR, double* gLp, double* gRp, double* qw) {
+  if (point_set != SGNB_POINTS_GLL && point_set != SGNB_POINTS_GAUSS)
+    return fail(nullptr, SGNB_ERR_INVALID, "point_set must be SGNB_POINTS_GLL or SGNB_POINTS_GAUSS");
+  FrTables t;
+  if (!fr_tables(P, t, point_set == SGNB_POINTS_GAUSS))
+    return fail(nullptr, SGNB_ERR_UNSUPPORTED, "P out of range");
+  const int n = P + 1;
+  if (nodes) std::memcpy(nodes, t.nodes, n * sizeof(double));
+  if (D) std::memcpy(D, t.D, n * n * sizeof(double));
+  if (lL) std::memcpy(lL, t.lL, n * sizeof(double));
+  if (lR) std::memcpy(lR, t.lR, n * sizeof(double));
+  if (gLp) std::memcpy(gLp, t.gLp, n * sizeof(double));
+  if (gRp) std::memcpy(gRp, t.gRp, n * sizeof(double));
+  if (qw) std::memcpy(qw, t.qw, n * sizeof(double));
+  return SGNB_OK;
+}
+
 int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* Hy,
                           double* HfaceX, double* HfaceY, double* HfaceXEnd,
                           double* HfaceYEnd) {
@@ -303,6 +349,10 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   *out = nullptr;
   int rc = check_desc(d);
   if (rc) return rc;
+  {  // argument errors (tables, point set against bathymetry) before device errors
+    FrTables t;
+    if ((rc = tables_for(d, t))) return rc;
+  }
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0)
@@ -376,6 +426,10 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   if (e == cudaSuccess) e = put(b.HfXEnd, c->C.HfXEnd);
   if (e == cudaSuccess) e = put(b.HfYEnd, c->C.HfYEnd);
   if (e != cudaSuccess) { cuda_fail(c, e, "upload of statics"); g_create_error = c->err; return bail(SGNB_ERR_CUDA); }
+  if (c->tab.gauss) {
+    e = cudaMalloc(&c->trbuf, 100 * (size_t)ne * sizeof(double));
+    if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(traces)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
+  }
   fill_consts(c);
 
   const size_t sbytes = (size_t)c->ntot * sizeof(double);
@@ -418,6 +472,7 @@ int sgnb_destroy(sgnb_ctx* c) {
   if (c->chunk) cudaGraphExecDestroy(c->chunk);
   if (c->evRead) cudaEventDestroy(c->evRead);
   cudaFree(c->Hbuf);
+  cudaFree(c->trbuf);
   for (int k = 0; k < 2; ++k) { cudaFree(c->U[k]); cudaFree(c->K1[k]); }
   cudaFree(c->K2);  // K3 lives in the same block
   cudaFree(c->partials); cudaFree(c->diag); cudaFree(c->dctrl); cudaFree(c->dtList);
@@ -841,6 +896,7 @@ extern "C" {
 
 int sgnb_set_ghosts(sgnb_ctx* c, const double* ghostL, const double* ghostR) {
   if (!c) return fail(c, SGNB_ERR_INVALID, "NULL context");
+  if (c->tab.gauss) return fail(c, SGNB_ERR_UNSUPPORTED, "Gauss points run on whole meshes");
   if (c->mixed) return fail(c, SGNB_ERR_UNSUPPORTED, "slab edges run in the FP64 modes");
   c->C.ghostL = ghostL;
   c->C.ghostR = ghostR;
@@ -1079,6 +1135,9 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
       return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances run without Manning friction");
     if (descs[i].Nx_global > 0)
       return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances are whole meshes");
+    if (descs[i].point_set != SGNB_POINTS_GLL ||
+        (descs[i].lL && descs[i].lL[0] != 1.0))
+      return bfail(nullptr, SGNB_ERR_UNSUPPORTED, "batched instances use GLL points");
     if (descs[i].device != descs[0].device)
       return bfail(nullptr, SGNB_ERR_INVALID, "all instances on one device");
   }

@@ -21,6 +21,7 @@ struct sgnb_ctx {
   long long Nd = 0, ntot = 0;
   sgnb::RhsConsts C{};
   double* Hbuf = nullptr;  // one allocation holding all statics
+  double* trbuf = nullptr;  // Gauss points: face traces, 4 faces x 5 fields x 5 ne
   double* U[2] = {nullptr, nullptr};
   // stage derivatives: FP64 (exact / fast) or FP32 (mixed precision)
   void* K1[2] = {nullptr, nullptr};

@@ -38,6 +38,12 @@ struct RhsConsts {
   // edge follows bcx (periodic wrap or wall)
   const double* ghostL;
   const double* ghostR;
+  // Gauss-Legendre points: face interpolation rows, and the face traces of every element
+  // formed by a pre-pass, [face: 0 left, 1 right, 2 bottom, 3 top][field][element][node]
+  double lL[5], lR[5];
+  double* tr;
+  int gauss;
+  int pad2_;
 };
 
 // Device-resident state of the adaptive integrator: the scalar loop variables of

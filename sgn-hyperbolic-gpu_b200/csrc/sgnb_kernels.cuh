@@ -240,6 +240,28 @@ __device__ __forceinline__ double flux_field(const TC& C, int v, double hn,
   }
 }
 
+// Face trace of one field along a line of solution points p[0], p[stride], ...:
+// sum_k l[k] p[k] accumulated from 0.0 in the reference's order (sgn2d.cpp:141-177), each
+// product and sum rounded on its own in both arithmetic modes, so that the trace an
+// element forms of itself, the one its neighbour forms of it in the same tile and the
+// one the trace pre-pass stores agree bit for bit.
+__device__ __forceinline__ double face_trace(const double* l, const double* p, int stride) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) s = __dadd_rn(s, __dmul_rn(l[k], p[k * stride]));
+  return s;
+}
+
+// Mirror ghost of a face trace across a wall normal to DIR, written 0.0 + v and
+// 0.0 + (-v) for the normal discharge (the mirror element's trace in the reference's
+// doubled-domain picture).
+template <int DIR>
+__device__ __forceinline__ void mirror_trace(const double* own, double* ghost) {
+#pragma unroll
+  for (int v = 0; v < NV; ++v) ghost[v] = __dadd_rn(0.0, own[v]);
+  ghost[DIR == 0 ? 1 : 2] = __dadd_rn(0.0, -own[DIR == 0 ? 1 : 2]);
+}
+
 // The line computation shared by the row (DIR 0) and column (DIR 1) passes: nodal
 // fluxes, both Rusanov face fluxes with central depths, the element's own face fluxes,
 // the 5-point differentiation and the correction lift (src/solver/sgn2d.cpp:188-275
@@ -253,11 +275,15 @@ __device__ __forceinline__ double flux_field(const TC& C, int v, double hn,
 // derivative of node m, then emit(m, v, d, q) with the FR-corrected derivative of flux
 // field v at node m (both already divided by J). The flux of each field is rebuilt from
 // per-node quantities inside the contraction, which keeps the live set small.
-template <bool EXACT, int DIR, class TC, class TB, class EmitH, class Emit>
+// GAUSS (Gauss-Legendre points): the own traces are interpolated with the rows lL / lR
+// of Tb, nLo / nHi are the neighbours' traces, and a wall (mirLo / mirHi) mirrors the own
+// trace.
+template <bool EXACT, int DIR, bool GAUSS = false, class TC, class TB, class EmitH, class Emit>
 __device__ __forceinline__ void line_pass(const TC& C, const TB& Tb, const double (&Un)[NP][NV],
                                           const double (&Hn)[NP], const double* nLo,
                                           const double* nHi, double HfLo, double HfHi,
-                                          EmitH&& emit_dh, Emit&& emit) {
+                                          EmitH&& emit_dh, Emit&& emit, bool mirLo = false,
+                                          bool mirHi = false) {
   Prim<EXACT> q[NP];
   double hn[NP], fn[NP];
 #pragma unroll
@@ -268,18 +294,38 @@ __device__ __forceinline__ void line_pass(const TC& C, const TB& Tb, const doubl
   }
   // face traces: own side t*, neighbour side s*
   double tLo[NV], tHi[NV], sLo[NV], sHi[NV];
+  if constexpr (GAUSS) {
 #pragma unroll
-  for (int v = 0; v < NV; ++v) {
-    tLo[v] = canon<EXACT>(Un[0][v]);
-    tHi[v] = canon<EXACT>(Un[NP - 1][v]);
-    sLo[v] = canon<EXACT>(nLo[v]);
-    sHi[v] = canon<EXACT>(nHi[v]);
+    for (int v = 0; v < NV; ++v) {
+      tLo[v] = face_trace(Tb.lL, &Un[0][v], NV);
+      tHi[v] = face_trace(Tb.lR, &Un[0][v], NV);
+    }
+    if (mirLo) {
+      mirror_trace<DIR>(tLo, sLo);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sLo[v] = nLo[v];
+    }
+    if (mirHi) {
+      mirror_trace<DIR>(tHi, sHi);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sHi[v] = nHi[v];
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      tLo[v] = canon<EXACT>(Un[0][v]);
+      tHi[v] = canon<EXACT>(Un[NP - 1][v]);
+      sLo[v] = canon<EXACT>(nLo[v]);
+      sHi[v] = canon<EXACT>(nHi[v]);
+    }
   }
   double jLo[NV], jHi[NV];  // common flux minus own face flux
   {
     const Prim<EXACT> qsLo(sLo), qsHi(sHi);
     Prim<EXACT> qtLo, qtHi;
-    if constexpr (EXACT) {
+    if constexpr (EXACT || GAUSS) {
       qtLo = Prim<EXACT>(tLo);
       qtHi = Prim<EXACT>(tHi);
     } else {
@@ -391,11 +437,12 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
   ghost[DIR == 0 ? 1 : 2] = -own[DIR == 0 ? 1 : 2];
 }
 
+
 // One tile of the fused right-hand side / stage kernel: tile (bx, by) of the mesh whose
 // constants are C, error partial slot blk. Shared by the single-instance kernel and the
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
 template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false,
-          bool GHOST = false>
+          bool GHOST = false, bool GAUSS = false>
 __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_, EXACT>::Smem& S) {
@@ -531,11 +578,20 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       hq[u] = ok ? q : -1;
       hg[u] = (GHOST && hs[u]) ? (long long)v * Ny * NP + (long long)(ey0 + (slot < TY ? slot : slot - TY)) * NP + t
                                : (long long)v * Nd + e * NPP + node;
+      if constexpr (GAUSS) {
+        // the neighbour's trace on the shared face: the left neighbour's right face (1),
+        // the right neighbour's left face (0), the bottom one's top face (3), the top
+        // one's bottom face (2)
+        const int f = slot < TY ? 1 : (slot < 2 * TY ? 0 : (slot < 2 * TY + TX ? 3 : 2));
+        hg[u] = ((long long)(f * NV + v) * (Nd / NPP) + e) * NP + t;
+      }
     }
 #pragma unroll
     for (int u = 0; u < NHIT; ++u)
       if (hq[u] >= 0) {
-        if constexpr (GHOST)
+        if constexpr (GAUSS)
+          hv[u] = C.tr[hg[u]];
+        else if constexpr (GHOST)
           hv[u] = hs[u] == 0 ? stage_value<MODE>(I, hg[u]) : (hs[u] == 1 ? C.ghostL : C.ghostR)[hg[u]];
         else
           hv[u] = stage_value<MODE>(I, hg[u]);
@@ -645,18 +701,24 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     double nLo[NV], nHi[NV];
     if (iy > 0) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nLo[v] = S.U[v][i - TX][j + NP * (NP - 1)];
+      for (int v = 0; v < NV; ++v) {
+        if constexpr (GAUSS) nLo[v] = face_trace(Tb.lR, &S.U[v][i - TX][j], NP);
+        else nLo[v] = S.U[v][i - TX][j + NP * (NP - 1)];
+      }
     } else if (wallB) {
-      mirror<1>(Un[0], nLo);
+      if constexpr (!GAUSS) mirror<1>(Un[0], nLo);
     } else {
 #pragma unroll
       for (int v = 0; v < NV; ++v) nLo[v] = T::halo_at(S, v, 2 * TY + ix, j);
     }
     if (iy + 1 < TYv) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nHi[v] = S.U[v][i + TX][j];
+      for (int v = 0; v < NV; ++v) {
+        if constexpr (GAUSS) nHi[v] = face_trace(Tb.lL, &S.U[v][i + TX][j], NP);
+        else nHi[v] = S.U[v][i + TX][j];
+      }
     } else if (wallT) {
-      mirror<1>(Un[NP - 1], nHi);
+      if constexpr (!GAUSS) mirror<1>(Un[NP - 1], nHi);
     } else {
 #pragma unroll
       for (int v = 0; v < NV; ++v) nHi[v] = T::halo_at(S, v, 2 * TY + TX + ix, j);
@@ -664,7 +726,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     const double HfLo = T::hf_y(S, i, j);
     const double HfHi = (iy + 1 < TYv) ? T::hf_y(S, i + TX, j) : T::hf_yt(S, ix, j);
     double by[NP];  // ncpY, -c^2 v h_y (sgn_flux2d.h:156-161)
-    line_pass<EXACT, 1>(
+    line_pass<EXACT, 1, GAUSS>(
         C, Tb, Un, Hn, nLo, nHi, HfLo, HfHi,
         [&](int b, double dh, const Prim<EXACT>& q) {
           if constexpr (EXACT) S.G[NV][i][j + NP * b] = C.mc2 * q.v * dh;
@@ -673,7 +735,8 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
         [&](int b, int v, double d, const Prim<EXACT>&) {
           if constexpr (EXACT) S.G[v][i][j + NP * b] = d;
           else S.G[v][i][j + NP * b] = v == NV - 1 ? d + by[b] : d;
-        });
+        },
+        iy == 0 && wallB, iy + 1 >= TYv && wallT);
   }
   __syncthreads();
 
@@ -691,18 +754,24 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     double nLo[NV], nHi[NV];
     if (ix > 0) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nLo[v] = S.U[v][i - 1][(NP - 1) + NP * j];
+      for (int v = 0; v < NV; ++v) {
+        if constexpr (GAUSS) nLo[v] = face_trace(Tb.lR, &S.U[v][i - 1][NP * j], 1);
+        else nLo[v] = S.U[v][i - 1][(NP - 1) + NP * j];
+      }
     } else if (wallL) {
-      mirror<0>(Un[0], nLo);
+      if constexpr (!GAUSS) mirror<0>(Un[0], nLo);
     } else {
 #pragma unroll
       for (int v = 0; v < NV; ++v) nLo[v] = T::halo_at(S, v, iy, j);
     }
     if (ix + 1 < TXv) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) nHi[v] = S.U[v][i + 1][NP * j];
+      for (int v = 0; v < NV; ++v) {
+        if constexpr (GAUSS) nHi[v] = face_trace(Tb.lL, &S.U[v][i + 1][NP * j], 1);
+        else nHi[v] = S.U[v][i + 1][NP * j];
+      }
     } else if (wallR) {
-      mirror<0>(Un[NP - 1], nHi);
+      if constexpr (!GAUSS) mirror<0>(Un[NP - 1], nHi);
     } else {
 #pragma unroll
       for (int v = 0; v < NV; ++v) nHi[v] = T::halo_at(S, v, TY + iy, j);
@@ -710,7 +779,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     const double HfLo = T::hf_x(S, i, j);
     const double HfHi = (ix + 1 < TXv) ? T::hf_x(S, i + 1, j) : T::hf_xr(S, iy, j);
     double dhx[NP];
-    line_pass<EXACT, 0>(
+    line_pass<EXACT, 0, GAUSS>(
         C, Tb, Un, Hn, nLo, nHi, HfLo, HfHi,
         [&](int a, double dh, const Prim<EXACT>&) { dhx[a] = dh; },
         [&](int a, int v, double d, const Prim<EXACT>& q) {
@@ -749,7 +818,8 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             }
           }
           S.G[v][i][loc] = res;
-        });
+        },
+        ix == 0 && wallL, ix + 1 >= TXv && wallR);
   }
   __syncthreads();
 
@@ -861,13 +931,55 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 // FRIC: Manning friction compiled in (instantiated only for contexts that use it, so the
 // frictionless kernels carry none of its code).
 // GHOST: slab edges compiled in (only contexts with ghost arrays launch these variants).
-template <int MODE, bool EXACT, bool FRIC = false, bool GHOST = false>
+// GAUSS: Gauss-Legendre points (after k_traces of the same stage).
+template <int MODE, bool EXACT, bool FRIC = false, bool GHOST = false, bool GAUSS = false>
 __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using T = Tile<8, 4, EXACT>;
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
-  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC, GHOST>(C, C, A, blockIdx.x, blockIdx.y,
+  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC, GHOST, GAUSS>(C, C, A, blockIdx.x, blockIdx.y,
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
+}
+
+// Face traces of every element for Gauss-Legendre points (sgn2d.cpp:141-177), of the
+// stage input the fused kernel of the same MODE reads: one thread per (direction,
+// element, transverse node), five fields, both faces. Writes C.tr. The traces are
+// explicitly rounded, so both arithmetic modes (EXACT) form the same bits.
+template <int MODE, bool EXACT>
+__global__ void __launch_bounds__(256) k_traces(const RhsConsts C, const StageArgs A) {
+  const long long ne = (long long)C.Nx * C.Ny;
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 2 * ne * NP) return;
+  StageIn I;
+  I.in = A.in;
+  I.dt = 0.0;
+  I.acoef = 0.0;
+  int cur = 0;
+  if constexpr (MODE != MODE_RHS) {
+    if (A.ctrl->done) return;
+    cur = A.ctrl->cur;
+    I.dt = A.ctrl->dt;
+    I.acoef = A.coef * I.dt;
+  }
+  I.u = A.U[cur];
+  I.k = A.kin_k2 ? A.K2 : A.K1[cur];
+  I.k1 = A.K1[cur];
+  I.k2 = A.K2;
+  I.k3 = A.K3;
+  const int dir = (int)(q / (ne * NP));
+  const long long r = q - dir * ne * NP;
+  const long long e = r / NP;
+  const int t = (int)(r % NP);
+  const int fl = dir == 0 ? 0 : 2;  // left / bottom face; the right / top one is fl + 1
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double line[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+      line[k] = stage_value<MODE>(I, (long long)v * C.Nd + e * NPP + (dir == 0 ? k + NP * t : t + NP * k));
+    C.tr[((long long)(fl * NV + v) * ne + e) * NP + t] = face_trace(C.lL, line, 1);
+    C.tr[((long long)((fl + 1) * NV + v) * ne + e) * NP + t] = face_trace(C.lR, line, 1);
+  }
 }
 
 // Batched form: one launch per stage walks the tiles of many independent instances

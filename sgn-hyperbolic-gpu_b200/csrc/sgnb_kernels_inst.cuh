@@ -12,6 +12,13 @@ template <int MODE>
 static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
   const dim3 grid((C.Nx + 7) / 8, (C.Ny + 3) / 4);
   const size_t smem = sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
+  if (C.gauss) {
+    const long long n = 2LL * C.Nx * C.Ny * NP;
+    k_traces<MODE, SGNB_EXACT><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(C, A);
+    if (C.manning) k_fused<MODE, SGNB_EXACT, true, false, true><<<grid, NTHR, smem, s>>>(C, A);
+    else k_fused<MODE, SGNB_EXACT, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
+    return cudaGetLastError();
+  }
   const bool ghost = C.ghostL != nullptr || C.ghostR != nullptr;
   if (C.manning) {
     if (ghost) k_fused<MODE, SGNB_EXACT, true, true><<<grid, NTHR, smem, s>>>(C, A);
@@ -23,17 +30,17 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
   return cudaGetLastError();
 }
 
-template <bool FRIC, bool GHOST>
+template <bool FRIC, bool GHOST, bool GAUSS = false>
 static cudaError_t prepare_variant() {
   const int bytes = (int)sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC, GHOST>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC, GHOST, GAUSS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC, GHOST>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC, GHOST, GAUSS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC, GHOST>,
+  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC, GHOST, GAUSS>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
@@ -42,6 +49,8 @@ static cudaError_t prepare_all() {
   if (e == cudaSuccess) e = prepare_variant<true, false>();
   if (e == cudaSuccess) e = prepare_variant<false, true>();
   if (e == cudaSuccess) e = prepare_variant<true, true>();
+  if (e == cudaSuccess) e = prepare_variant<false, false, true>();
+  if (e == cudaSuccess) e = prepare_variant<true, false, true>();
   return e;
 }
 

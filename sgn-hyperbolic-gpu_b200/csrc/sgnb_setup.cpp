@@ -1,4 +1,4 @@
-// sgnb_setup.cpp -- host-side set-up of the FR discretisation: GLL tables, node
+// sgnb_setup.cpp -- host-side set-up of the FR discretisation: FR tables, node
 // coordinates, and the bathymetry statics the kernels read.
 //
 // The arithmetic here must produce the same doubles as the reference's constructors
@@ -40,14 +40,9 @@ double legendre_deriv(int n, double x) {
   return n * (x * legendre(n, x) - legendre(n - 1, x)) / q;
 }
 
-}  // namespace
-
-bool fr_tables(int P, FrTables& t) {
-  if (P < 1 || P > 7) return false;
-  const int n = P + 1;
-  t.P = P;
-  // Gauss-Lobatto points: +-1 and the roots of L_P', found by Newton's method from
-  // the Chebyshev-Lobatto points; L_P'' comes from Legendre's equation.
+// Gauss-Lobatto points: +-1 and the roots of L_P', found by Newton's method from the
+// Chebyshev-Lobatto points; L_P'' comes from Legendre's equation.
+void gll_nodes(int P, FrTables& t) {
   t.nodes[0] = -1.0;
   t.nodes[P] = 1.0;
   for (int i = 1; i < P; ++i) {
@@ -62,6 +57,46 @@ bool fr_tables(int P, FrTables& t) {
     }
     t.nodes[i] = x;
   }
+}
+
+// Gauss-Legendre points: the n = P + 1 roots of L_n by Newton's method from the
+// asymptotic guesses -cos(pi (i + 3/4) / (n + 1/2)).
+void gauss_nodes(int P, FrTables& t) {
+  const int n = P + 1;
+  for (int i = 0; i < n; ++i) {
+    double x = -std::cos(kPi * (i + 0.75) / (n + 0.5));
+    for (int it = 0; it < 100; ++it) {
+      const double f = legendre(n, x);
+      const double fp = legendre_deriv(n, x);
+      const double step = f / fp;
+      x -= step;
+      if (std::fabs(step) < 1e-15) break;
+    }
+    t.nodes[i] = x;
+  }
+}
+
+// Lagrange basis polynomial j of the nodes x (barycentric weights bw) at xq: the
+// barycentric formula w_j / (xq - x_j) / sum_k w_k / (xq - x_k), and exactly the
+// Kronecker delta where xq is a node.
+double lagrange(int n, const double* x, const double* bw, int j, double xq) {
+  for (int k = 0; k < n; ++k)
+    if (std::fabs(xq - x[k]) < 1e-14) return (k == j) ? 1.0 : 0.0;
+  const double num = bw[j] / (xq - x[j]);
+  double den = 0.0;
+  for (int k = 0; k < n; ++k) den += bw[k] / (xq - x[k]);
+  return num / den;
+}
+
+}  // namespace
+
+bool fr_tables(int P, FrTables& t, bool gauss) {
+  if (P < 1 || P > 7) return false;
+  const int n = P + 1;
+  t.P = P;
+  t.gauss = gauss;
+  if (gauss) gauss_nodes(P, t);
+  else gll_nodes(P, t);
   // barycentric weights 1 / prod_{k != j} (x_j - x_k)
   double bw[8];
   for (int j = 0; j < n; ++j) {
@@ -82,10 +117,10 @@ bool fr_tables(int P, FrTables& t) {
     }
     t.D[i * n + i] = diag;
   }
-  // interpolation to the faces: with end-point nodes these are unit rows
+  // interpolation rows to the faces x = -1, +1 (unit rows for the end-point nodes of GLL)
   for (int j = 0; j < n; ++j) {
-    t.lL[j] = (j == 0) ? 1.0 : 0.0;
-    t.lR[j] = (j == P) ? 1.0 : 0.0;
+    t.lL[j] = lagrange(n, t.nodes, bw, j, -1.0);
+    t.lR[j] = lagrange(n, t.nodes, bw, j, +1.0);
   }
   // Huynh's g_DG correction functions gL = (-1)^P (L_P - L_{P+1})/2,
   // gR = (L_P + L_{P+1})/2, differentiated at the nodes
@@ -96,10 +131,18 @@ bool fr_tables(int P, FrTables& t) {
     t.gLp[i] = 0.5 * sgnP * (a - b);
     t.gRp[i] = 0.5 * (a + b);
   }
-  // Lobatto quadrature weights 2 / (P (P+1) L_P(x_i)^2)
-  for (int i = 0; i < n; ++i) {
-    const double lp = legendre(P, t.nodes[i]);
-    t.qw[i] = 2.0 / (P * (P + 1.0) * lp * lp);
+  if (gauss) {
+    // Gauss quadrature weights 2 / ((1 - x_i^2) L_{P+1}'(x_i)^2)
+    for (int i = 0; i < n; ++i) {
+      const double d = legendre_deriv(P + 1, t.nodes[i]);
+      t.qw[i] = 2.0 / ((1.0 - t.nodes[i] * t.nodes[i]) * d * d);
+    }
+  } else {
+    // Lobatto quadrature weights 2 / (P (P+1) L_P(x_i)^2)
+    for (int i = 0; i < n; ++i) {
+      const double lp = legendre(P, t.nodes[i]);
+      t.qw[i] = 2.0 / (P * (P + 1.0) * lp * lp);
+    }
   }
   return true;
 }

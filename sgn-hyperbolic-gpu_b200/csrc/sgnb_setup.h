@@ -5,9 +5,11 @@
 
 namespace sgnb {
 
-// FROperators1D for GLL points (src/core/fr_operators.h:57-115), degree P <= 7.
+// FROperators1D (src/core/fr_operators.h:57-115), degree P <= 7: Gauss-Lobatto points,
+// or Gauss-Legendre points (gauss; fr_operators.cpp:86-100).
 struct FrTables {
   int P = 0;
+  bool gauss = false;
   double nodes[8] = {}, D[64] = {}, lL[8] = {}, lR[8] = {}, gLp[8] = {}, gRp[8] = {}, qw[8] = {};
 };
 
@@ -27,7 +29,7 @@ struct Bathymetry {
   std::vector<double> Hnod, Hx, Hy, HfX, HfY, HfXEnd, HfYEnd;
 };
 
-bool fr_tables(int P, FrTables& t);
+bool fr_tables(int P, FrTables& t, bool gauss = false);
 double still_depth(int kind, const double* p, double x, double y);
 // number of doubles a parameter vector of this kind must hold (-1: unknown kind)
 int bathy_param_count(int kind, const double* p, int n);

@@ -28,6 +28,8 @@ LIB_PATH = os.path.join(HERE, "libsgnb.so")
 
 BC_PERIODIC = 0
 BC_WALL = 1
+POINTS_GLL = 0    # solution points (PointSet, src/core/fr_operators.h:51)
+POINTS_GAUSS = 1  # Gauss-Legendre: flat bottom only (BATHY_NONE), FP64 modes
 FP64_EXACT = 0
 FP64_FAST = 1
 MIXED = 2
@@ -67,7 +69,7 @@ class _Desc(C.Structure):
                 ("bathy_kind", C.c_int), ("bathy_par", _dp), ("n_bathy_par", C.c_int),
                 ("Hnod", _dp), ("Hx", _dp), ("Hy", _dp), ("HfaceX", _dp), ("HfaceY", _dp),
                 ("HfaceXEnd", _dp), ("HfaceYEnd", _dp),
-                ("Nx_global", C.c_int), ("ex_offset", C.c_int)]
+                ("Nx_global", C.c_int), ("ex_offset", C.c_int), ("point_set", C.c_int)]
 
 
 class _Opts(C.Structure):
@@ -140,6 +142,7 @@ SIGNATURES = {
     "sgnb_state_device_ptr": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p),
                                         C.POINTER(C.c_void_p)]),
     "sgnb_fr_tables": (C.c_int, [C.c_int] + [_dp] * 7),
+    "sgnb_fr_tables_points": (C.c_int, [C.c_int, C.c_int] + [_dp] * 7),
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
     "sgnb_set_ghosts": (C.c_int, [C.c_void_p, _dp, _dp]),
     "sgnb_slab_pack": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_void_p]),
@@ -209,13 +212,15 @@ def _check(rc: int, handle=None):
         raise SgnbError(rc, msg.decode() if msg else "")
 
 
-def fr_tables(P: int = 4) -> dict:
-    """FROperators1D tables built by the library's host set-up (no device needed)."""
+def fr_tables(P: int = 4, points: int = POINTS_GLL) -> dict:
+    """FROperators1D(P, pointSet) tables built by the library's host set-up (no device
+    needed)."""
     n = P + 1
     out = {k: np.zeros(n) for k in ("nodes", "lL", "lR", "gLp", "gRp", "qw")}
     out["D"] = np.zeros(n * n)
-    _check(lib().sgnb_fr_tables(P, *(_ptr(out[k]) for k in
-                                     ("nodes", "D", "lL", "lR", "gLp", "gRp", "qw"))))
+    _check(lib().sgnb_fr_tables_points(P, points, *(_ptr(out[k]) for k in
+                                                     ("nodes", "D", "lL", "lR", "gLp", "gRp",
+                                                      "qw"))))
     return out
 
 
@@ -223,10 +228,11 @@ class _DescHolder:
     """Builds an sgnb_desc and keeps the numpy arrays it points to alive."""
 
     def __init__(self, P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y, precision,
-                 device, bathy_kind, bathy_par, tables, bathy_arrays):
+                 device, bathy_kind, bathy_par, tables, bathy_arrays, points=POINTS_GLL):
         self.keep = []
         d = _Desc()
         lib().sgnb_desc_init(C.byref(d))
+        d.point_set = points
         d.P, d.Nx, d.Ny, d.Lx, d.Ly = P, Nx, Ny, float(Lx), float(Ly)
         d.g, d.c, d.gamma, d.nManning = float(g), float(c), float(gamma), float(nManning)
         d.bc_x, d.bc_y, d.precision, d.device = bc_x, bc_y, precision, device
@@ -287,12 +293,13 @@ class SGN2DB200:
     def __init__(self, P=4, Nx=8, Ny=6, Lx=10.0, Ly=8.0, g=9.81, c=0.0, gamma=1.5,
                  nManning=0.0, bc_x=BC_PERIODIC, bc_y=BC_PERIODIC, precision=FP64_EXACT,
                  device=0, bathy_kind=BATHY_NONE, bathy_par=(), tables=None,
-                 bathy_arrays=None, _handle=None):
+                 bathy_arrays=None, points=POINTS_GLL, _handle=None):
         self._h = None
         self._owned = _handle is None
         if _handle is None:
             holder = _DescHolder(P, Nx, Ny, Lx, Ly, g, c, gamma, nManning, bc_x, bc_y,
-                                 precision, device, bathy_kind, bathy_par, tables, bathy_arrays)
+                                 precision, device, bathy_kind, bathy_par, tables, bathy_arrays,
+                                 points)
             h = C.c_void_p()
             _check(lib().sgnb_create(C.byref(holder.desc), C.byref(h)))
         else:
@@ -303,6 +310,7 @@ class SGN2DB200:
         self.n = 5 * self.Nd
         self.precision = precision
         self.device = device
+        self.points = points
 
     def close(self):
         if self._h and self._owned:
@@ -537,7 +545,7 @@ class SGNBatch:
                 ("c", 0.0), ("gamma", 1.5), ("nManning", 0.0), ("bc_x", BC_PERIODIC),
                 ("bc_y", BC_PERIODIC), ("precision", FP64_FAST), ("device", 0),
                 ("bathy_kind", BATHY_NONE), ("bathy_par", ()), ("tables", None),
-                ("bathy_arrays", None))]
+                ("bathy_arrays", None), ("points", POINTS_GLL))]
             if kw:
                 raise TypeError(f"SGNBatch: unknown instance keys {sorted(kw)}")
             holders.append(_DescHolder(*args))

@@ -48,6 +48,35 @@ def test_fr_tables_bitwise():
         assert bits_equal(mine[k], ref[k]), k
 
 
+def test_gauss_tables_bitwise(golden):
+    """FROperators1D(4, GaussLegendre): the reference's tables, committed as fixtures."""
+    mine = sgnb.fr_tables(4, points=sgnb.POINTS_GAUSS)
+    for k in ("nodes", "D", "lL", "lR", "gLp", "gRp", "qw"):
+        assert bits_equal(mine[k], golden[f"gauss_{k}"]), k
+    with pytest.raises(sgnb.SgnbError) as ei:
+        sgnb.fr_tables(4, points=3)
+    assert ei.value.status == 1
+
+
+def test_gauss_points_need_a_flat_bottom():
+    """SGN2D refuses bathymetry with non-GLL points (sgn2d.cpp:46-47): SGNB_ERR_INVALID,
+    before any device is touched; the flat bottom sets up all-zero statics."""
+    with pytest.raises(sgnb.SgnbError) as ei:
+        sgnb.SGN2DB200(Nx=8, Ny=6, points=sgnb.POINTS_GAUSS, bathy_kind=sgnb.BATHY_CONST,
+                       bathy_par=(1.0,))
+    assert ei.value.status == 1
+    with pytest.raises(sgnb.SgnbError) as ei:
+        sgnb.SGN2DB200(Nx=8, Ny=6, points=sgnb.POINTS_GAUSS, precision=sgnb.MIXED)
+    assert ei.value.status == 2
+    h = sgnb._DescHolder(4, 8, 6, 10.0, 8.0, 9.81, 0.0, 1.5, 0.0, 0, 0, sgnb.FP64_EXACT, 0,
+                         sgnb.BATHY_NONE, (), None, None, sgnb.POINTS_GAUSS)
+    import ctypes as C
+
+    out = [np.ones(n) for n in (1200, 1200, 1200, 240, 240, 30, 40)]
+    assert sgnb.lib().sgnb_setup_bathymetry(C.byref(h.desc), *(sgnb._ptr(a) for a in out)) == 0
+    assert all(not a.any() for a in out)
+
+
 KINDS = [
     (O.BATHY_NONE, ()),
     (O.BATHY_CONST, (1.0,)),
