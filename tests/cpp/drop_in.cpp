@@ -8,7 +8,9 @@
 //   1. the device rhs equals SGN2D::rhs bit for bit (exact mode);
 //   2. lake at rest: max |rhs| < 1e-12;
 //   3. an adaptive run (tEnd 0.3, atol 1e-10, rtol 1e-8) takes the CPU's accepted /
-//      rejected steps, ends within 1e-10 relative of the CPU state and conserves mass.
+//      rejected steps, ends within 1e-10 relative of the CPU state and conserves mass;
+//   4. a host solver on Gauss-Legendre points (flat bottom): its tables reach the device
+//      through the same constructor, and the device rhs equals SGN2D::rhs bit for bit.
 // Prints one line per check and exits non-zero on any failure.
 #include "sgnb.hpp"
 
@@ -97,6 +99,32 @@ int main() {
     report(diff / scale < 1e-10, "adaptive run: state vs CPU (relative)", diff / scale);
     const double dM = std::fabs(host.mass(Ug) - host.mass(U)) / std::fabs(host.mass(U));
     report(dM < 1e-13, "adaptive run: mass conserved", dM);
+  }
+  {  // 4. Gauss-Legendre points on a flat bottom (H = 0)
+    sgn::SGN2D gauss(4, 7, 5, 8.75, 6.5, par, {}, sgn::PointSet::GaussLegendre);
+    std::vector<double> xg, yg;
+    gauss.nodeCoords(xg, yg);
+    const int Ng = gauss.nDof();
+    std::vector<double> hg(Ng), ug(Ng), vg(Ng), wg(Ng), pg(Ng);
+    for (int i = 0; i < Ng; ++i) {
+      hg[i] = 1.0 + 0.04 * std::sin(2 * kPi * xg[i] / 8.75) * std::cos(2 * kPi * yg[i] / 6.5);
+      ug[i] = 0.08 * std::cos(2 * kPi * xg[i] / 8.75);
+      vg[i] = -0.05 * std::sin(2 * kPi * yg[i] / 6.5);
+      wg[i] = 0.02 * std::sin(xg[i]);
+      pg[i] = 0.01 * std::cos(yg[i]);
+    }
+    const sgn::State Ug = gauss.makeState(hg, ug, vg, wg, pg);
+    sgn::State Rc, Rg;
+    gauss.rhs(Ug, Rc);
+    sgnb::SGN2DB200 dev(gauss);
+    dev.upload(Ug);
+    dev.rhsOnce(Rg);
+    const bool same = Rc.size() == Rg.size() &&
+                      std::memcmp(Rc.data(), Rg.data(), Rc.size() * sizeof(double)) == 0;
+    double diff = 0.0;
+    for (size_t i = 0; i < Rc.size() && i < Rg.size(); ++i)
+      diff = std::fmax(diff, std::fabs(Rc[i] - Rg[i]));
+    report(same, "Gauss points: device rhs == SGN2D::rhs bit for bit", diff);
   }
   std::printf(failures ? "%d FAILED\n" : "ALL PASSED\n", failures);
   return failures ? 1 : 0;
