@@ -216,6 +216,12 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
                           double* HfaceX, double* HfaceY, double* HfaceXEnd,
                           double* HfaceYEnd);
 
+/* The fast mode's reciprocal (fn 0: 1/x) and square root (fn 1) elementwise over n
+ * doubles of device memory (x in, y out) on `stream` (NULL: the legacy default stream),
+ * synchronised: the fast arithmetic mode's own Newton-Raphson forms, exposed so that
+ * tests can compare them with the IEEE results. */
+int sgnb_fast_math(int fn, const double* x, double* y, long long n, void* stream);
+
 /* Slab decomposition (the reference's multi-GPU solver, src/cuda/sgn2d_cuda_mpi.cu:148-161,
  * 487-537: x slabs, one halo exchange per right-hand side, one reduction of the error norm
  * per step). A slab is a context created with Nx_global / ex_offset; its neighbours'

@@ -894,6 +894,15 @@ int batch_run(sgnb_batch* b) {
 
 extern "C" {
 
+int sgnb_fast_math(int fn, const double* x, double* y, long long n, void* stream) {
+  if ((fn != 0 && fn != 1) || n < 0 || (n > 0 && (!x || !y)))
+    return fail(nullptr, SGNB_ERR_INVALID, "fn 0 or 1, device arrays x, y of n doubles");
+  cudaError_t e = dev::launch_fast_math(fn, x, y, n, (cudaStream_t)stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(nullptr, SGNB_ERR_CUDA, cudaGetErrorString(e));
+  return SGNB_OK;
+}
+
 int sgnb_set_ghosts(sgnb_ctx* c, const double* ghostL, const double* ghostR) {
   if (!c) return fail(c, SGNB_ERR_INVALID, "NULL context");
   if (c->tab.gauss) return fail(c, SGNB_ERR_UNSUPPORTED, "Gauss points run on whole meshes");

@@ -167,6 +167,9 @@ namespace dev {
 cudaError_t launch_mixed_batch(int mode, int blocks, const BatchArgsM& B, cudaStream_t s);
 cudaError_t prepare_mixed_batch();
 
+// The fast mode's reciprocal (fn 0) and square root (fn 1) elementwise, for tests.
+cudaError_t launch_fast_math(int fn, const double* x, double* y, long long n, cudaStream_t s);
+
 // Slab edges: the stage inputs of the first and last element columns' edge nodes
 // (a = 0 / a = 4), [field][row][node], for the neighbours' ghosts. mode 0: rhs of in;
 // 1: intermediate stage (kin_k2, coef of A); 2: end-point candidate.

@@ -156,8 +156,8 @@ __device__ __forceinline__ double canon(double v) {
 
 // Reciprocal for the fast mode: the hardware estimate (PTX rcp.approx.ftz.f64) refined by
 // two Newton-Raphson steps r <- r + r (1 - x r), each of which doubles the number of
-// correct bits. Accurate to a few ulp for the positive normal depths it is used on; the
-// library's self-test compares it with IEEE 1/x.
+// correct bits. For normal x (the positive depths and error scales it is used on); the
+// GPU tests compare it with IEEE 1/x in ulps through sgnb_fast_math.
 __device__ __forceinline__ double fast_rcp(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -166,6 +166,23 @@ __device__ __forceinline__ double fast_rcp(double x) {
   e = fma(-x, r, 1.0);
   r = fma(r, e, r);
   return r;
+}
+
+// Square root for the fast mode, by Newton-Raphson on the reciprocal square root: the
+// hardware estimate y of 1/sqrt(x) (PTX rsqrt.approx.ftz.f64), two steps
+// y <- y (3/2 - (x/2) y^2), then s = x y and one Newton (Heron) step on s^2 = x written
+// with the residual, s <- s + (y/2) (x - s^2). Normal finite x only; zero, subnormal,
+// infinite, negative and NaN arguments take the IEEE square root. Tested against IEEE
+// sqrt in ulps through sgnb_fast_math.
+__device__ __forceinline__ double fast_sqrt(double x) {
+  if (!(x >= 2.2250738585072014e-308 && x <= 1.7976931348623157e308)) return sqrt(x);
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double hx = 0.5 * x;
+  y = y * fma(-hx * y, y, 1.5);
+  y = y * fma(-hx * y, y, 1.5);
+  const double s = x * y;
+  return fma(0.5 * y, fma(-s, s, x), s);
 }
 
 // Primitive variables u, v, w, p of one point (src/physics/sgn_flux2d.h:92-93).
@@ -222,7 +239,7 @@ template <bool EXACT, int DIR, class TC>
 __device__ __forceinline__ double wave_speed(const TC& C, const double* U,
                                              const Prim<EXACT>& q) {
   const double arg = C.g * U[0] + q.p + C.c2;
-  const double ce = sqrt(arg > 0.0 ? arg : 0.0);
+  const double ce = EXACT ? sqrt(arg > 0.0 ? arg : 0.0) : fast_sqrt(arg > 0.0 ? arg : 0.0);
   return fabs(DIR == 0 ? q.u : q.v) + ce;
 }
 
@@ -877,15 +894,22 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
           if (okk[u]) {
             const double k4 = (&S.G[v][0][0])[sof[u]];
             outp[(long long)v * Nd + gof[u]] = k4;
-            // scaled embedded error, src/solver/rk.cpp:118-128
+            // scaled embedded error, src/solver/rk.cpp:118-128; the candidate uNew is
+            // still in the tile (the passes only read S.U)
             const double dt = I.dt;
-            const double un = fsal_finish(uu[u], fsal_part(c1[u], c2[u]), c3[u], dt);
+            const double un = (&S.U[v][0][0])[sof[u]];
             const double uEmb = uu[u] + dt * (7.0 / 24.0 * c1[u] + 0.25 * c2[u] + 1.0 / 3.0 * c3[u] +
                                               0.125 * k4);
             const double e = un - uEmb;
             const double au = fabs(uu[u]), an = fabs(un);
             const double sc = atol + rtol * (au < an ? an : au);
-            const double rr = e / sc;
+            double rr;
+            if constexpr (EXACT) {
+              rr = e / sc;
+            } else {
+              // the fast mode's reciprocal (a few ulp) where sc is a normal number
+              rr = sc >= 2.2250738585072014e-308 ? e * fast_rcp(sc) : e / sc;
+            }
             esum += rr * rr;
             const double ar = fabs(rr);
             emax = emax < ar ? ar : emax;

@@ -11,6 +11,19 @@ cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A, 
 }
 cudaError_t prepare_fused_fast() { return prepare_all(); }
 
+// The fast mode's reciprocal (fn 0) and square root (fn 1) on a device array, for tests.
+__global__ void k_fast_math(int fn, const double* __restrict__ x, double* __restrict__ y,
+                            long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = fn == 0 ? fast_rcp(x[i]) : fast_sqrt(x[i]);
+}
+
+cudaError_t launch_fast_math(int fn, const double* x, double* y, long long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_fast_math<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(fn, x, y, n);
+  return cudaGetLastError();
+}
+
 // Slab edges: one thread per (side, field, row, transverse node). Side 0 reads the first
 // element column's left nodes (a = 0) into sendL, side 1 the last column's right nodes
 // (a = P) into sendR; both [field][row][node]. The stage inputs are formed with the same

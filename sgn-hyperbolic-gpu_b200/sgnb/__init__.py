@@ -144,6 +144,7 @@ SIGNATURES = {
     "sgnb_fr_tables": (C.c_int, [C.c_int] + [_dp] * 7),
     "sgnb_fr_tables_points": (C.c_int, [C.c_int, C.c_int] + [_dp] * 7),
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
+    "sgnb_fast_math": (C.c_int, [C.c_int, _dp, _dp, C.c_longlong, C.c_void_p]),
     "sgnb_set_ghosts": (C.c_int, [C.c_void_p, _dp, _dp]),
     "sgnb_slab_pack": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_void_p]),
     "sgnb_slab_begin": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
