@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include "sgnb_device.h"
+#include "sgnb_fastmath.cuh"
 
 namespace sgnb {
 namespace mix {
@@ -628,7 +629,8 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           const double e = un - uEmb;
           const double au = fabs(uu[u]), an = fabs(un);
           const double sc = atol + rtol * (au < an ? an : au);
-          const double rr = e / sc;
+          // the fast reciprocal (a few ulp) where sc is a normal number
+          const double rr = sc >= 2.2250738585072014e-308 ? e * dev::fast_rcp(sc) : e / sc;
           esum += rr * rr;
           const double ar = fabs(rr);
           emax = emax < ar ? ar : emax;
