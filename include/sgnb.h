@@ -255,6 +255,24 @@ int sgnb_slab_partials(sgnb_ctx* ctx, double** partials, int* nblk);
 int sgnb_slab_control(sgnb_ctx* ctx, const double* partials, int nblk, long long n_total,
                       void* stream);
 int sgnb_slab_status(sgnb_ctx* ctx, sgnb_rk_stats* st, int* done, void* stream);
+/* Fused edge exchange (the slab form of the multi-GPU solver's RHS epilogue writing the
+ * halo line into the peer's ghost buffer): one stage launch with this stage's ghost inputs
+ * (ghostL / ghostR, NULL at a wall), whose slab-edge tiles of stages 2 and 3 also store
+ * the next stage's edge inputs straight into the neighbours' ghost arrays for that stage
+ * (edgeL: the left neighbour's right ghost, edgeR: the right neighbour's left ghost; on
+ * another device, peer memory that this device can address). Stage 1 and 4 write no edges;
+ * the caller packs stage 0 and 2 (sgnb_slab_pack, with the neighbours' ghost arrays as
+ * the send buffers) and orders each launch after the neighbours' launches that fill its
+ * ghosts. */
+int sgnb_slab_stage(sgnb_ctx* ctx, int stage, const double* ghostL, const double* ghostR,
+                    double* edgeL, double* edgeR, void* stream);
+/* Lets kernels on `device` address the memory of `peer` (NVLink / NVSwitch peer access;
+ * a repeated call is a no-op; device == peer is a no-op). */
+int sgnb_enable_peer_access(int device, int peer);
+/* The controller on the error partials of all nslab (<= 32) slabs, read in place in slab
+ * order (partials[k]: device pointer, peer memory allowed; nblk[k] blocks): no gather. */
+int sgnb_slab_control_all(sgnb_ctx* ctx, const double* const* partials, const int* nblk,
+                          int nslab, long long n_total, void* stream);
 
 /* Device-side sampling for the reference's applications, which download the whole state
  * at every sample time and scan it on the host (apps/shoal_focus_mpi.cu:195-205,

@@ -987,6 +987,67 @@ int sgnb_slab_launch(sgnb_ctx* c, int stage, void* stream) {
   return SGNB_OK;
 }
 
+int sgnb_slab_stage(sgnb_ctx* c, int stage, const double* ghostL, const double* ghostR,
+                    double* edgeL, double* edgeR, void* stream) {
+  if (!c || stage < 1 || stage > 4) return fail(c, SGNB_ERR_INVALID, "stage 1..4");
+  if (c->mixed || c->tab.gauss)
+    return fail(c, SGNB_ERR_UNSUPPORTED, "slab edges run in the FP64 modes on GLL points");
+  if ((edgeL && !ghostL) || (edgeR && !ghostR))
+    return fail(c, SGNB_ERR_INVALID, "an edge output needs the neighbour's ghost input");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  if (c->chunk) {  // captured launches hold other constants
+    cudaGraphExecDestroy(c->chunk);
+    c->chunk = nullptr;
+    c->chunkLen = 0;
+  }
+  c->C.ghostL = ghostL;
+  c->C.ghostR = ghostR;
+  const bool fused = stage == 2 || stage == 3;  // the next stage's inputs are known
+  c->C.edgeL = fused ? edgeL : nullptr;
+  c->C.edgeR = fused ? edgeR : nullptr;
+  cudaError_t e;
+  if (stage == 1) e = launch(c, rhs_launch(c->U[c->cur], (double*)c->K1[c->cur]), s);
+  else e = launch(c, stage_launch(stage), s);
+  c->C.edgeL = c->C.edgeR = nullptr;
+  SGNB_CU(c, e);
+  return SGNB_OK;
+}
+
+int sgnb_slab_control_all(sgnb_ctx* c, const double* const* partials, const int* nblk, int nslab,
+                          long long n_total, void* stream) {
+  if (!c || !partials || !nblk || nslab < 1 || nslab > dev::kMaxSlabs || n_total < 1)
+    return fail(c, SGNB_ERR_INVALID, "1..32 slabs, their partials and block counts");
+  if (int rc = set_device(c)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  dev::SlabPartials L{};
+  L.ns = nslab;
+  L.start[0] = 0;
+  for (int k = 0; k < nslab; ++k) {
+    if (!partials[k] || nblk[k] < 1) return fail(c, SGNB_ERR_INVALID, "bad partials");
+    L.p[k] = partials[k];
+    L.start[k + 1] = L.start[k] + nblk[k];
+  }
+  SGNB_CU(c, dev::launch_controller_slabs(c->dctrl, L, n_total, s));
+  return SGNB_OK;
+}
+
+int sgnb_enable_peer_access(int device, int peer) {
+  if (device == peer) return SGNB_OK;
+  int can = 0;
+  cudaError_t e = cudaDeviceCanAccessPeer(&can, device, peer);
+  if (e != cudaSuccess) return fail(nullptr, SGNB_ERR_CUDA, cudaGetErrorString(e));
+  if (!can) return fail(nullptr, SGNB_ERR_UNSUPPORTED, "the devices cannot address each other");
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(nullptr, SGNB_ERR_CUDA, cudaGetErrorString(e));
+  e = cudaDeviceEnablePeerAccess(peer, 0);
+  if (e == cudaErrorPeerAccessAlreadyEnabled) {
+    cudaGetLastError();  // clear the sticky-free status of the repeated call
+    e = cudaSuccess;
+  }
+  if (e != cudaSuccess) return fail(nullptr, SGNB_ERR_CUDA, cudaGetErrorString(e));
+  return SGNB_OK;
+}
+
 int sgnb_slab_partials(sgnb_ctx* c, double** partials, int* nblk) {
   if (!c || !partials || !nblk) return fail(c, SGNB_ERR_INVALID, "NULL argument");
   *partials = c->partials;

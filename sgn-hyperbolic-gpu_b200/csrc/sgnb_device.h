@@ -38,6 +38,12 @@ struct RhsConsts {
   // edge follows bcx (periodic wrap or wall)
   const double* ghostL;
   const double* ghostR;
+  // fused edge exchange of the intermediate stages: the next stage's inputs at the slab's
+  // edge nodes, written by this launch into the neighbours' ghost arrays (the left
+  // neighbour's right ghost, the right neighbour's left ghost; another device's memory in
+  // a multi-device run); NULL: none
+  double* edgeL;
+  double* edgeR;
   // Gauss-Legendre points: face interpolation rows, and the face traces of every element
   // formed by a pre-pass, [face: 0 left, 1 right, 2 bottom, 3 top][field][element][node]
   double lL[5], lR[5];
@@ -169,6 +175,17 @@ cudaError_t prepare_mixed_batch();
 
 // The fast mode's reciprocal (fn 0) and square root (fn 1) elementwise, for tests.
 cudaError_t launch_fast_math(int fn, const double* x, double* y, long long n, cudaStream_t s);
+
+// Error partials of every slab of a decomposed mesh, in slab order: slab s holds blocks
+// start[s] .. start[s+1]-1 at p[s] (3 doubles per block).
+constexpr int kMaxSlabs = 32;
+struct SlabPartials {
+  const double* p[kMaxSlabs];
+  long long start[kMaxSlabs + 1];
+  int ns;
+};
+cudaError_t launch_controller_slabs(CtrlState* c, const SlabPartials& L, long long n,
+                                    cudaStream_t s);
 
 // Slab edges: the stage inputs of the first and last element columns' edge nodes
 // (a = 0 / a = 4), [field][row][node], for the neighbours' ghosts. mode 0: rhs of in;

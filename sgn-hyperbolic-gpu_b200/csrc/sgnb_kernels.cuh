@@ -892,6 +892,38 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       }
     }
   }
+  if constexpr (GHOST && MODE == MODE_STAGE) {
+    // Fused edge exchange: the slab-edge tiles form the next stage's input at their edge
+    // nodes (a = 0 of the first column, a = 4 of the last) from this launch's result and
+    // store it straight into the neighbours' ghost arrays, [field][row][node], while the
+    // other tiles still compute. After stage 2 (k1 added) that is u + 3/4 dt k2, the next
+    // launch's own stage input; after stage 3 the end-point candidate. Both with the
+    // explicitly rounded combinations of the stage inputs, so the neighbour sees the bits
+    // this slab's own next launch forms.
+    const bool outLo = C.edgeL != nullptr && ex0 == 0, outHi = C.edgeR != nullptr && ex0 + TXv == Nx;
+    if (outLo || outHi) {
+      const volatile CtrlState* vc = A.ctrl;
+      const int cr = vc->cur;
+      const double dt = vc->dt;
+      const double* __restrict__ u0 = A.U[cr];
+      const double* __restrict__ k1 = A.K1[cr];
+      const double* __restrict__ k2 = A.K2;
+      const int per = NV * TYv * NP;
+      for (int q = tid; q < 2 * per; q += NTHR) {
+        const int side = q / per;
+        if (side == 0 ? !outLo : !outHi) continue;
+        const int r = q - side * per;
+        const int t = r % NP, iy = (r / NP) % TYv, v = r / (NP * TYv);
+        const int ixe = side == 0 ? 0 : TXv - 1;
+        const int node = (side == 0 ? 0 : NP - 1) + NP * t;
+        const long long g = (long long)v * Nd + ((long long)(ex0 + ixe) + (long long)Nx * (ey0 + iy)) * NPP + node;
+        const double kout = S.G[v][TX * iy + ixe][node];
+        const double val = A.kin_k2 == 0 ? stage_axpy(u0[g], 0.75 * dt, kout)
+                                          : fsal_finish(u0[g], fsal_part(k1[g], k2[g]), kout, dt);
+        (side == 0 ? C.edgeL : C.edgeR)[(long long)v * Ny * NP + (long long)(ey0 + iy) * NP + t] = val;
+      }
+    }
+  }
   if constexpr (MODE == MODE_FSAL) {
     // deterministic block reduction: fixed shuffle tree, then warps in order
 #pragma unroll

@@ -20,16 +20,19 @@ __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b 
 // accept if the RMS scaled error <= 1 (rk.cpp:129-142), PI update clamped to
 // [facMin, facMax] (:148-152), dtMin abort (:155-160), and the loop test and the
 // end-time clip of the next attempt (:95-97).
-__device__ __forceinline__ void controller_block(CtrlState* c, const double* partials, int nblk,
-                                                 long long n) {
+// row(b): the three partials (sum r^2, max |r|, NaN count) of error block b.
+template <class Row>
+__device__ __forceinline__ void controller_core(CtrlState* c, const Row& row, long long nblk,
+                                                long long n) {
   __shared__ double ss[kCtrlThreads], sm[kCtrlThreads], sn[kCtrlThreads];
   if (c->done) return;
   const int t = threadIdx.x;
   double s = 0.0, m = 0.0, nn = 0.0;
-  for (int b = t; b < nblk; b += kCtrlThreads) {
-    s += partials[3 * b + 0];
-    m = dmax(m, partials[3 * b + 1]);
-    nn += partials[3 * b + 2];
+  for (long long b = t; b < nblk; b += kCtrlThreads) {
+    const double* r = row(b);
+    s += r[0];
+    m = dmax(m, r[1]);
+    nn += r[2];
   }
   ss[t] = s;
   sm[t] = m;
@@ -100,9 +103,28 @@ __device__ __forceinline__ void controller_block(CtrlState* c, const double* par
   if (c->t + c->dt > tEnd) c->dt = tEnd - c->t;
 }
 
+__device__ __forceinline__ void controller_block(CtrlState* c, const double* partials, int nblk,
+                                                 long long n) {
+  controller_core(c, [&](long long b) { return partials + 3 * b; }, nblk, n);
+}
+
 __global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const double* partials,
                                                              int nblk, long long n) {
   controller_block(c, partials, nblk, n);
+}
+
+// Slab controller: the error blocks of every slab of a decomposed mesh, read in place (on
+// other devices: peer loads) in slab order, as one list.
+__global__ void __launch_bounds__(kCtrlThreads) k_controller_slabs(CtrlState* c, const SlabPartials L,
+                                                                   long long n) {
+  controller_core(
+      c,
+      [&](long long b) {
+        int s = 0;
+        while (s + 1 < L.ns && b >= L.start[s + 1]) ++s;
+        return L.p[s] + 3 * (b - L.start[s]);
+      },
+      L.start[L.ns], n);
 }
 
 // Batched controller: block i runs instance i's controller on its own partials.
@@ -161,6 +183,12 @@ __global__ void __launch_bounds__(256) k_diag(int what, const RhsConsts C, const
 cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk, long long n,
                               cudaStream_t s) {
   k_controller<<<1, kCtrlThreads, 0, s>>>(c, partials, nblk, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_controller_slabs(CtrlState* c, const SlabPartials& L, long long n,
+                                    cudaStream_t s) {
+  k_controller_slabs<<<1, kCtrlThreads, 0, s>>>(c, L, n);
   return cudaGetLastError();
 }
 

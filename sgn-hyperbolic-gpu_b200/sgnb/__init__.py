@@ -153,6 +153,10 @@ SIGNATURES = {
     "sgnb_slab_launch": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "sgnb_slab_partials": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.POINTER(C.c_int)]),
     "sgnb_slab_control": (C.c_int, [C.c_void_p, _dp, C.c_int, C.c_longlong, C.c_void_p]),
+    "sgnb_slab_stage": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, C.c_void_p]),
+    "sgnb_enable_peer_access": (C.c_int, [C.c_int, C.c_int]),
+    "sgnb_slab_control_all": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.POINTER(C.c_int), C.c_int,
+                                        C.c_longlong, C.c_void_p]),
     "sgnb_slab_status": (C.c_int, [C.c_void_p, C.POINTER(_Stats), C.POINTER(C.c_int),
                                    C.c_void_p]),
     "sgnb_eta_max": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,

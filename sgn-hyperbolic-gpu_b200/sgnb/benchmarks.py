@@ -288,7 +288,7 @@ def run_slabs(args, clock_sampler, peak):
     of the final states."""
     import torch
 
-    from .slabs import SlabSolver
+    from .slabs import PeerSlabSolver, SlabSolver
 
     Nx, Ny = W.CFG2["Nx"], W.CFG2["Ny"]
     if args.mesh:
@@ -341,6 +341,26 @@ def run_slabs(args, clock_sampler, peak):
                                  accepted=st.accepted, rejected=st.rejected,
                                  rel_diff_vs_whole=rel(s.download_tensor(), ref))
             clocks = clk.summary()
+    # the fused edge exchange: stage kernels store the neighbours' ghosts, controllers read
+    # every slab's partials in place; one stream per slab (ordered by events) or one shared
+    fused = {}
+    for n in (2, 4):
+        for mode in ("per-slab", "shared"):
+            with PeerSlabSolver(kw, nslabs=n, streams=mode) as s:
+                s.upload_tensor(Ud)
+                s.integrate_steps(0.0, dt0, args.warmup)
+                s.upload_tensor(Ud)
+                e0, e1 = _events(torch, s.stream)
+                torch.cuda.synchronize()
+                e0.record(s.stream)
+                st = s.integrate_steps(0.0, dt0, args.steps)
+                e1.record(s.stream)
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / 1e3
+                fused[f"{n} {mode}"] = dict(value=dof * st.rhsEvals / t,
+                                           ms_per_step=t / args.steps * 1e3,
+                                           accepted=st.accepted, rejected=st.rejected,
+                                           rel_diff_vs_whole=rel(s.download_tensor(), ref))
     top = slabs["4"]
     edge_bytes = 5 * Ny * 5 * 8
     line = {
@@ -354,7 +374,7 @@ def run_slabs(args, clock_sampler, peak):
                    "edge_bytes": edge_bytes,
                    "exchange_bytes_per_attempt_per_slab": 3 * 2 * edge_bytes,
                    "l2": f"inputs larger than L2 ({8 * 5 * dof / 1e9:.1f} GB per state)"},
-        "whole_mesh": whole, "slabs": slabs,
+        "whole_mesh": whole, "slabs": slabs, "fused_exchange": fused,
         "slab_over_whole": {k: v["value"] / whole["value"] for k, v in slabs.items()},
         "clocks": clocks, "roofline": None, "gpu_launches": None,
         "timing": "CUDA events on the solver's stream around the K steps (the host launches "

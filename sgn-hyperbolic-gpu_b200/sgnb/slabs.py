@@ -245,6 +245,9 @@ class SlabSolver:
             s.close()
         self.slabs = []
 
+    def _sync(self):
+        self.torch.cuda.synchronize(self.device)
+
     def __enter__(self):
         return self
 
@@ -269,10 +272,10 @@ class SlabSolver:
         if t.dtype != torch.float64 or t.numel() != NV * 25 * self.Nx * self.Ny:
             raise ValueError("SlabSolver.upload_tensor: float64 whole-mesh state expected")
         v = t.reshape(NV, self.Ny, self.Nx, 25)
-        torch.cuda.synchronize(self.device)
+        self._sync()
         for s in self.slabs:
             s.ctx.state_tensor().view(NV, self.Ny, s.nx, 25).copy_(v[:, :, s.ex0:s.ex0 + s.nx, :])
-        torch.cuda.synchronize(self.device)
+        self._sync()
 
     def download_tensor(self):
         """The whole mesh's state as a new device tensor (single process)."""
@@ -281,10 +284,10 @@ class SlabSolver:
             raise ValueError("SlabSolver.download_tensor: one slab per rank")
         out = torch.empty((NV, self.Ny, self.Nx, 25), dtype=torch.float64,
                           device=f"cuda:{self.device}")
-        torch.cuda.synchronize(self.device)
+        self._sync()
         for s in self.slabs:
             out[:, :, s.ex0:s.ex0 + s.nx, :].copy_(s.ctx.state_tensor().view(NV, self.Ny, s.nx, 25))
-        torch.cuda.synchronize(self.device)
+        self._sync()
         return out.reshape(-1)
 
     def download_local(self):
@@ -384,6 +387,216 @@ class SlabSolver:
                     break
         for s in self.slabs:
             _check(lib().sgnb_slab_status(s.h, C.byref(st), C.byref(done), C.c_void_p(sp)), s.h)
+        if st.status == 4:
+            raise SgnbError(4, "non-finite state in a slab integration")
+        if not done.value:
+            raise SgnbError(6, "slab integration did not finish within its attempt limit")
+        return _stats(st)
+
+
+class PeerSlabSolver(SlabSolver):
+    """Slabs with the fused edge exchange: no send buffers and no copies.
+
+    Every slab has a ghost array per side for each stage that reads ghosts (1: the FSAL
+    head, 2, 3, 4). The packs of stages 0 and 2 (after the controller has set dt) and the
+    edge tiles of the stage-2 and stage-3 kernels store the next stage's edge inputs
+    straight into the neighbours' ghost arrays (sgnb_slab_stage), and each slab's
+    controller reads every slab's error partials in place (sgnb_slab_control_all). Slabs
+    may sit on several devices (``devices``, slab r on devices[r % len]): the stores and
+    loads then cross NVLink as peer accesses, and every launch that reads ghosts or partials
+    waits, through events, for the neighbours' launches that wrote them (and every end-point
+    launch for all controllers of the previous attempt, which still read its partials).
+    ``streams="shared"`` runs every slab on one stream (single device only)."""
+
+    STAGES = (1, 2, 3, 4)
+
+    def __init__(self, kw: dict, nslabs: int = 1, devices=None, streams: str = "per-slab"):
+        import torch
+
+        self.torch = torch
+        self.kw = dict(kw)
+        self.Nx = int(kw["Nx"])
+        self.Ny = int(kw["Ny"])
+        self.periodic = int(kw.get("bc_x", 0)) == 0
+        self.devices = list(devices) if devices else [0]
+        if streams not in ("shared", "per-slab"):
+            raise ValueError("streams: 'shared' or 'per-slab'")
+        if streams == "shared" and len(set(self.devices)) > 1:
+            raise ValueError("a shared stream needs a single device")
+        if nslabs > 32:
+            raise ValueError("PeerSlabSolver: at most 32 slabs")
+        self.device = self.devices[0]
+        self.size = nslabs
+        self.ranks = list(range(nslabs))
+        self.parts = [slab_partition(self.Nx, nslabs, r) for r in range(nslabs)]
+        self.links = [neighbours(r, nslabs, self.periodic) for r in range(nslabs)]
+        self.exchange = None
+        for a in set(self.devices):
+            for b in set(self.devices):
+                _check(lib().sgnb_enable_peer_access(a, b))
+        self.slabs = []
+        self.ghost = []  # ghost[r][stage] = (left, right) tensors on slab r's device
+        try:
+            for r in range(nslabs):
+                dev = self.devices[r % len(self.devices)]
+                a, w = self.parts[r]
+                s = _Slab(kw, self.Nx, a, w, dev, torch)
+                s.device = dev
+                self.slabs.append(s)
+                n = NV * self.Ny * NP
+                self.ghost.append({st: (torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}"),
+                                        torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}"))
+                                   for st in self.STAGES})
+        except Exception:
+            self.close()
+            raise
+        self.n_total = 5 * 25 * self.Nx * self.Ny
+        if streams == "shared":
+            sh = torch.cuda.Stream(self.device)
+            self.streams = [sh] * nslabs
+        else:
+            self.streams = [torch.cuda.Stream(s.device) for s in self.slabs]
+        self.shared = streams == "shared"
+        self.stream = self.streams[0]
+        self._pp = (_dp * nslabs)(*[C.cast(C.c_void_p(s.partials.data_ptr()), _dp)
+                                    for s in self.slabs])
+        self._nb = (C.c_int * nslabs)(*[s.nblk for s in self.slabs])
+        self._sync()
+
+    def _sync(self):
+        for d in set(self.devices):
+            self.torch.cuda.synchronize(d)
+
+    # --- ghost pointers ------------------------------------------------------------
+    def _ghosts_in(self, r, st):
+        """(left, right) ghost inputs of slab r for stage st (None at a wall)."""
+        left, right = self.links[r]
+        gl, gr = self.ghost[r][st]
+        return (_dev(gl.data_ptr()) if left is not None else None,
+                _dev(gr.data_ptr()) if right is not None else None)
+
+    def _edges_out(self, r, st):
+        """Where slab r's edges go for stage st: its left edge into the left neighbour's
+        right ghost, its right edge into the right neighbour's left ghost."""
+        left, right = self.links[r]
+        return (_dev(self.ghost[left][st][1].data_ptr()) if left is not None else None,
+                _dev(self.ghost[right][st][0].data_ptr()) if right is not None else None)
+
+    # --- ordering between slabs ----------------------------------------------------
+    def _record(self, r):
+        if self.shared:
+            return None
+        e = self.torch.cuda.Event()
+        e.record(self.streams[r])
+        return e
+
+    def _wait(self, r, events):
+        if self.shared:
+            return
+        for e in events:
+            if e is not None:
+                self.streams[r].wait_event(e)
+
+    def _nbr_events(self, r, ev):
+        left, right = self.links[r]
+        return [ev[q] for q in (left, right) if q is not None and q != r]
+
+    def _pack(self, st_in, st_out, in_ptrs=None):
+        """Packs of stage st_in (0 or 2) into the neighbours' ghosts of stage st_out."""
+        ev = []
+        for r, s in enumerate(self.slabs):
+            oL, oR = self._edges_out(r, st_out)
+            # a wall side writes nowhere: a scratch ghost of this slab takes it
+            sc = self.ghost[r][st_out]
+            sendL = oL if oL is not None else _dev(sc[0].data_ptr())
+            sendR = oR if oR is not None else _dev(sc[1].data_ptr())
+            _check(lib().sgnb_slab_pack(s.h, st_in, _dev(None if in_ptrs is None else in_ptrs[r]),
+                                        sendL, sendR, C.c_void_p(self.streams[r].cuda_stream)), s.h)
+            ev.append(self._record(r))
+        return ev
+
+    def _stage(self, st, prev_ev, extra=None):
+        ev = []
+        for r, s in enumerate(self.slabs):
+            self._wait(r, self._nbr_events(r, prev_ev) + (extra or []))
+            gL, gR = self._ghosts_in(r, st)
+            oL, oR = self._edges_out(r, st + 1) if st in (2, 3) else (None, None)
+            _check(lib().sgnb_slab_stage(s.h, st, gL, gR, oL, oR,
+                                         C.c_void_p(self.streams[r].cuda_stream)), s.h)
+            ev.append(self._record(r))
+        return ev
+
+    # --- right-hand side ---------------------------------------------------------
+    def rhs(self, U):
+        torch = self.torch
+        ins = [torch.from_numpy(self._cols(U, s.ex0, s.nx)).to(f"cuda:{s.device}") for s in self.slabs]
+        outs = [torch.empty_like(t) for t in ins]
+        self._sync()
+        ev = self._pack(0, 1, [t.data_ptr() for t in ins])
+        for r, (s, t, o) in enumerate(zip(self.slabs, ins, outs)):
+            self._wait(r, self._nbr_events(r, ev))
+            gL, gR = self._ghosts_in(r, 1)
+            _check(lib().sgnb_set_ghosts(s.h, gL, gR), s.h)
+            s.ctx.rhs_device(t.data_ptr(), o.data_ptr(), self.streams[r].cuda_stream)
+        self._sync()
+        dU = np.empty((NV, self.Ny, self.Nx, 25))
+        for r, o in enumerate(outs):
+            a, w = self.parts[r]
+            dU[:, :, a:a + w, :] = o.cpu().numpy().reshape(NV, self.Ny, w, 25)
+        return dU.reshape(-1)
+
+    def upload(self, U):
+        self._sync()
+        for s in self.slabs:
+            s.ctx.upload(self._cols(U, s.ex0, s.nx))
+        self._sync()
+
+    def download_local(self):
+        self._sync()
+        return {r: s.ctx.download() for r, s in enumerate(self.slabs)}
+
+    # --- BS3(2) ------------------------------------------------------------------
+    def _run(self, t0, tEnd, dt0, nsteps, opt, dts, check_every, limit):
+        """Per attempt: the stage-2 pack, stages 2, 3 (their edge tiles fill the
+        neighbours' ghosts of the next stage), 4, and every slab's controller on all slabs'
+        partials in place."""
+        o = _Opts(**dataclasses.asdict(opt or AdaptiveRKOptions()))
+        d = None if dts is None else np.ascontiguousarray(dts, dtype=np.float64)
+        self._sync()
+        for s in self.slabs:
+            _check(lib().sgnb_slab_begin(s.h, float(t0), float(tEnd), float(dt0), int(nsteps),
+                                         None if d is None else d.ctypes.data_as(_dp),
+                                         C.byref(o)), s.h)
+        ev = self._pack(0, 1)
+        ev = self._stage(1, ev)
+        ctrl_ev = []
+        attempts = 0
+        done = C.c_int(0)
+        st = _Stats()
+        while True:
+            ev = self._pack(2, 2)
+            ev = self._stage(2, ev)
+            ev = self._stage(3, ev)
+            # the end-point launch overwrites this slab's partials: every controller of
+            # the previous attempt has read them
+            fsal_ev = self._stage(4, ev, extra=ctrl_ev)
+            ctrl_ev = []
+            for r, s in enumerate(self.slabs):
+                self._wait(r, fsal_ev)
+                _check(lib().sgnb_slab_control_all(s.h, self._pp, self._nb, self.size, self.n_total,
+                                                   C.c_void_p(self.streams[r].cuda_stream)), s.h)
+                ctrl_ev.append(self._record(r))
+            attempts += 1
+            if attempts % check_every == 0 or attempts >= limit:
+                s0 = self.slabs[0]
+                _check(lib().sgnb_slab_status(s0.h, C.byref(st), C.byref(done),
+                                              C.c_void_p(self.streams[0].cuda_stream)), s0.h)
+                if done.value or attempts >= limit:
+                    break
+        self._sync()
+        for r, s in enumerate(self.slabs):
+            _check(lib().sgnb_slab_status(s.h, C.byref(st), C.byref(done),
+                                          C.c_void_p(self.streams[r].cuda_stream)), s.h)
         if st.status == 4:
             raise SgnbError(4, "non-finite state in a slab integration")
         if not done.value:

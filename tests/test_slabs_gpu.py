@@ -145,3 +145,50 @@ def test_adaptive_to_end_time(bc):
         # a run that starts at its end time takes no step
         st0 = s.integrate_adaptive(tEnd, tEnd, dt0)
         assert st0.accepted == 0 and st0.rejected == 0
+
+
+# ---------------------------------------------------------------------------- fused exchange
+from sgnb.slabs import PeerSlabSolver  # noqa: E402
+
+
+@pytest.mark.parametrize("streams", ["shared", "per-slab"])
+@pytest.mark.parametrize("bc", [0, 1])
+@pytest.mark.parametrize("nslabs", [1, 2, 3, 4])
+def test_fused_exchange_frozen_replay_bitwise(streams, bc, nslabs):
+    """Stage kernels storing the next stage's edge inputs into the neighbours' ghosts, the
+    controller reading all slabs' partials in place: the whole mesh's bs3 steps bit for
+    bit, with every slab on one stream or each on its own (concurrent) stream."""
+    kw, U = shoal_case(bc, Nx=13, Ny=6)
+    kw = dict(kw, precision=sgnb.FP64_EXACT)
+    with sgnb.SGN2DB200(**kw) as d:
+        d.upload(U)
+        R = d.rhs(U)
+        dt0 = d.cfl_time_step(0.4)
+        n = 9
+        dts = dt0 * (1.0 + 0.2 * np.cos(np.arange(n)))
+        d.bs3_steps(0.0, dts)
+        ref = d.download()
+    with PeerSlabSolver(kw, nslabs=nslabs, streams=streams) as s:
+        assert bits_equal(s.rhs(U), R)
+        s.upload(U)
+        st = s.integrate_steps(0.0, dts[0], n, dts=dts, check_every=2)
+        assert st.accepted == n and st.rejected == 0
+        assert bits_equal(s.download(), ref)
+
+
+@pytest.mark.parametrize("streams", ["shared", "per-slab"])
+def test_fused_exchange_adaptive(streams):
+    kw, U = bump_case(1, Nx=16, Ny=6)
+    kw = dict(kw, precision=sgnb.FP64_FAST)
+    with sgnb.SGN2DB200(**kw) as d:
+        d.upload(U)
+        dt0 = d.cfl_time_step(0.5)
+        tEnd = 11.5 * dt0
+        st1 = d.integrate_adaptive(0.0, tEnd, dt0)
+        ref = d.download()
+    with PeerSlabSolver(kw, nslabs=4, streams=streams) as s:
+        s.upload(U)
+        st = s.integrate_adaptive(0.0, tEnd, dt0, check_every=3)
+        assert (st.accepted, st.rejected) == (st1.accepted, st1.rejected)
+        assert abs(st.tReached - tEnd) <= 1e-14 * tEnd
+        assert rel_per_field(s.download(), ref) < 1e-10
