@@ -202,61 +202,75 @@ void fill_consts(sgnb_ctx* c) {
   C.tr = c->trbuf;
 }
 
-int build_chunk_graph(sgnb_ctx* c, int len) {
-  if (c->chunk && c->chunkLen == len) return SGNB_OK;
-  if (c->chunk) {
-    cudaGraphExecDestroy(c->chunk);
-    c->chunk = nullptr;
-  }
+// The device-side loop: a CUDA graph whose one node is a WHILE conditional node; its body
+// is one attempt (stages 2, 3, the end-point stage, the controller), and the controller
+// sets the condition. One graph launch runs attempts until the run is done or attemptCap
+// is reached, with no host round trip and no attempt launched after the end.
+int build_loop_graph(sgnb_ctx* c) {
+  if (c->chunk) return SGNB_OK;
   cudaGraph_t g = nullptr;
-  SGNB_CU(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = cudaSuccess;
-  for (int k = 0; k < len && e == cudaSuccess; ++k) {
-    e = launch(c, stage_launch(2), c->stream);  // k2 = R(u + dt/2 k1)
-    if (e != cudaSuccess) break;
-    e = launch(c, stage_launch(3), c->stream);  // k3 = R(u + 3dt/4 k2)
-    if (e != cudaSuccess) break;
-    e = launch(c, stage_launch(4), c->stream);  // uNew, k4 = R(uNew), error partials
-    if (e != cudaSuccess) break;
-    e = dev::launch_controller(c->dctrl, c->partials, c->nblk, c->ntot, c->stream);
+  SGNB_CU(c, cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle loop;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = loop;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_fail(c, e, "conditional node of the device-side loop");
   }
-  cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
-  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "capture of the attempt chunk"); }
-  if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
-  e = cudaGraphInstantiate(&c->chunk, g, 0);
+  cudaGraph_t body = p.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    e = launch(c, stage_launch(2), c->stream);                 // k2 = R(u + dt/2 k1)
+    if (e == cudaSuccess) e = launch(c, stage_launch(3), c->stream);  // k3 = R(u + 3dt/4 k2)
+    if (e == cudaSuccess) e = launch(c, stage_launch(4), c->stream);  // uNew, k4, partials
+    if (e == cudaSuccess)
+      e = dev::launch_controller_loop(c->dctrl, c->partials, c->nblk, c->ntot, loop, c->stream);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &body);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&c->chunk, g, 0);
   cudaGraphDestroy(g);
-  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
-  c->chunkLen = len;
+  if (e != cudaSuccess) {
+    c->chunk = nullptr;
+    return cuda_fail(c, e, "device-side loop graph");
+  }
+  c->chunkLen = 1;
   return SGNB_OK;
 }
 
-// Drive the device-resident loop until the controller reports done.
+// Drive the device-side loop until the controller reports done: each graph launch runs up
+// to kAttemptsPerLaunch attempts (a bound on one launch's duration); the host reads the
+// controller state between launches.
 int run_loop(sgnb_ctx* c) {
-  const int len = 16;
-  int rc = build_chunk_graph(c, len);
+  constexpr long long kAttemptsPerLaunch = 4096;
+  int rc = build_loop_graph(c);
   if (rc) return rc;
+  CtrlState& h = *c->hctrl;
+  h.attemptCap = h.attempts + kAttemptsPerLaunch;
   SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
   // kernels per right-hand side: the fused kernel, after the trace pre-pass for Gauss points
   const long long per_rhs = c->tab.gauss ? 2 : 1, per_attempt = 3 * per_rhs + 1;
-  c->launches = per_rhs + per_attempt * len;  // head + the first chunk
+  const long long attempts0 = h.attempts;
   // FSAL head: k1 = R(u) into K1[cur] (FP32 in the mixed mode)
   SGNB_CU(c, launch(c, rhs_launch(c->U[c->cur], c->mixed ? nullptr : (double*)c->K1[c->cur]),
                     c->stream));
-  // two chunks in flight: enqueue chunk k+1 before waiting for chunk k's readback
-  SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
-  SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
-  SGNB_CU(c, cudaEventRecord(c->evRead, c->stream));
-  for (long long guard = 0;; ++guard) {
+  for (;;) {
     SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
-    c->launches += per_attempt * len;
-    SGNB_CU(c, cudaEventSynchronize(c->evRead));
-    if (c->hctrl->done) break;
     SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
-    SGNB_CU(c, cudaEventRecord(c->evRead, c->stream));
+    SGNB_CU(c, cudaStreamSynchronize(c->stream));
+    if (h.done) break;
+    h.attemptCap = h.attempts + kAttemptsPerLaunch;  // more attempts than one launch allows
+    SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
   }
-  SGNB_CU(c, cudaStreamSynchronize(c->stream));
-  SGNB_CU(c, cudaMemcpy(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost));
-  c->cur = c->hctrl->cur;
+  c->launches = per_rhs + per_attempt * (h.attempts - attempts0);
+  c->cur = h.cur;
   return SGNB_OK;
 }
 

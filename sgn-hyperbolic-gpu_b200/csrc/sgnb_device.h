@@ -68,6 +68,7 @@ struct CtrlState {
   double* log;           // attempt log: (t, dt, errNorm, accepted) per attempt
   long long logCap;      // capacity of the log in attempts
   long long maxAccepted; // > 0: stop after this many accepted steps
+  long long attemptCap;  // the device-side loop hands back to the host at this attempt count
 };
 
 // Buffers of one fused launch.
@@ -228,6 +229,11 @@ size_t fused_smem_bytes();
 
 // Controller of one adaptive attempt: deterministic reduction of the per-CTA error
 // partials, accept/reject, PI step-size update and the next attempt's dt.
+// The controller as the last node of the body of a device-side WHILE loop (a conditional
+// node of a CUDA graph): it also sets the loop condition, false once the run is done or
+// the attempt count has reached attemptCap.
+cudaError_t launch_controller_loop(CtrlState* c, const double* partials, int nblk, long long n,
+                                   cudaGraphConditionalHandle loop, cudaStream_t s);
 cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk,
                               long long n, cudaStream_t s);
 // Largest eta = h - H inside a window, with its node: (value, index) per block.

@@ -113,6 +113,16 @@ __global__ void __launch_bounds__(kCtrlThreads) k_controller(CtrlState* c, const
   controller_block(c, partials, nblk, n);
 }
 
+// The controller of the device-side loop: one attempt's decision, then the WHILE node's
+// condition for the next pass of the body (one block; thread 0 wrote the state).
+__global__ void __launch_bounds__(kCtrlThreads) k_controller_loop(CtrlState* c, const double* partials,
+                                                                  int nblk, long long n,
+                                                                  cudaGraphConditionalHandle loop) {
+  controller_block(c, partials, nblk, n);
+  if (threadIdx.x == 0)
+    cudaGraphSetConditional(loop, (c->done == 0 && c->attempts < c->attemptCap) ? 1u : 0u);
+}
+
 // Slab controller: the error blocks of every slab of a decomposed mesh, read in place (on
 // other devices: peer loads) in slab order, as one list.
 __global__ void __launch_bounds__(kCtrlThreads) k_controller_slabs(CtrlState* c, const SlabPartials L,
@@ -183,6 +193,12 @@ __global__ void __launch_bounds__(256) k_diag(int what, const RhsConsts C, const
 cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk, long long n,
                               cudaStream_t s) {
   k_controller<<<1, kCtrlThreads, 0, s>>>(c, partials, nblk, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_controller_loop(CtrlState* c, const double* partials, int nblk, long long n,
+                                   cudaGraphConditionalHandle loop, cudaStream_t s) {
+  k_controller_loop<<<1, kCtrlThreads, 0, s>>>(c, partials, nblk, n, loop);
   return cudaGetLastError();
 }
 
