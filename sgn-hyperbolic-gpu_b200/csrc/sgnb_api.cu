@@ -755,8 +755,9 @@ struct sgnb_batch {
   long long ntiles[3] = {0, 0, 0};
   int shape = 0;                       // tuned tile shape
   int blocks = 0;                      // tuned persistent grid
-  cudaGraphExec_t chunk = nullptr;
+  cudaGraphExec_t chunk = nullptr;     // the device-side loop of the tuned configuration
   int chunkShape = -1, chunkBlocks = -1;
+  int* dcount = nullptr;               // [2] running instances, finished controller blocks
   cudaEvent_t evRead = nullptr;
   long long launches = 0;
   std::string err;
@@ -795,26 +796,44 @@ BatchArgs batch_args(sgnb_batch* b, int shape, int kin_k2, double coef) {
   return B;
 }
 
-int batch_build_graph(sgnb_batch* b, int len) {
+// The batch's device-side loop: a WHILE conditional node whose body is one attempt of
+// every instance (three batched stage launches and the batched loop controller, which
+// keeps the loop going while any instance runs).
+int batch_build_graph(sgnb_batch* b) {
   if (b->chunk && b->chunkShape == b->shape && b->chunkBlocks == b->blocks) return SGNB_OK;
   if (b->chunk) { cudaGraphExecDestroy(b->chunk); b->chunk = nullptr; }
   cudaGraph_t g = nullptr;
-  SGNB_BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = cudaSuccess;
-  for (int k = 0; k < len && e == cudaSuccess; ++k) {
-    e = batch_launch(b, 1, b->shape, b->blocks, 0, 0.5);
-    if (e == cudaSuccess) e = batch_launch(b, 1, b->shape, b->blocks, 1, 0.75);
-    if (e == cudaSuccess) e = batch_launch(b, 2, b->shape, b->blocks, 0, 0.0);
-    if (e == cudaSuccess)
-      e = dev::launch_controller_batch(b->dctrl, b->dpart, b->dnblk[b->shape], b->dntot, b->n,
-                                       b->stream);
+  SGNB_BCU(b, cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle loop;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = loop;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+  if (e == cudaSuccess) {
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      e = batch_launch(b, 1, b->shape, b->blocks, 0, 0.5);
+      if (e == cudaSuccess) e = batch_launch(b, 1, b->shape, b->blocks, 1, 0.75);
+      if (e == cudaSuccess) e = batch_launch(b, 2, b->shape, b->blocks, 0, 0.0);
+      if (e == cudaSuccess)
+        e = dev::launch_controller_batch_loop(b->dctrl, b->dpart, b->dnblk[b->shape], b->dntot,
+                                              b->n, b->dcount, loop, b->stream);
+      cudaError_t e2 = cudaStreamEndCapture(b->stream, &body);
+      if (e == cudaSuccess) e = e2;
+    }
   }
-  cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
-  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return bfail(b, SGNB_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorName(e)); }
-  if (e2 != cudaSuccess) return bfail(b, SGNB_ERR_CUDA, "batch cudaStreamEndCapture");
-  e = cudaGraphInstantiate(&b->chunk, g, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->chunk, g, 0);
   cudaGraphDestroy(g);
-  if (e != cudaSuccess) return bfail(b, SGNB_ERR_CUDA, "batch cudaGraphInstantiate");
+  if (e != cudaSuccess) {
+    b->chunk = nullptr;
+    return bfail(b, SGNB_ERR_CUDA, std::string("batch loop graph: ") + cudaGetErrorName(e));
+  }
   b->chunkShape = b->shape;
   b->chunkBlocks = b->blocks;
   return SGNB_OK;
@@ -880,26 +899,29 @@ int batch_prepare(sgnb_batch* b) {
   return SGNB_OK;
 }
 
-// Controllers already initialised in b->hctrl; runs until every instance is done.
+// Controllers already initialised in b->hctrl; runs until every instance is done, each
+// graph launch up to 4096 attempts (a bound on one launch; the host then relaunches).
 int batch_run(sgnb_batch* b) {
-  const int len = 8;
-  if (int rc = batch_build_graph(b, len)) return rc;
+  constexpr long long kAttemptsPerLaunch = 4096;
+  if (int rc = batch_build_graph(b)) return rc;
+  long long a0 = 0;
+  for (int i = 0; i < b->n; ++i) {
+    b->hctrl[i].attemptCap = b->hctrl[i].attempts + kAttemptsPerLaunch;
+    a0 = std::max(a0, b->hctrl[i].attempts);
+  }
   if (int rc = batch_prepare(b)) return rc;
   SGNB_BCU(b, batch_launch(b, 0, b->shape, b->blocks, 0, 0.0));
-  b->launches = 1 + 4LL * len;
-  SGNB_BCU(b, cudaGraphLaunch(b->chunk, b->stream));
-  SGNB_BCU(b, cudaMemcpyAsync(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost, b->stream));
-  SGNB_BCU(b, cudaEventRecord(b->evRead, b->stream));
   for (;;) {
     SGNB_BCU(b, cudaGraphLaunch(b->chunk, b->stream));
-    b->launches += 4LL * len;
-    SGNB_BCU(b, cudaEventSynchronize(b->evRead));
-    if (all_done(b)) break;
     SGNB_BCU(b, cudaMemcpyAsync(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost, b->stream));
-    SGNB_BCU(b, cudaEventRecord(b->evRead, b->stream));
+    SGNB_BCU(b, cudaStreamSynchronize(b->stream));
+    if (all_done(b)) break;
+    for (int i = 0; i < b->n; ++i) b->hctrl[i].attemptCap = b->hctrl[i].attempts + kAttemptsPerLaunch;
+    SGNB_BCU(b, cudaMemcpyAsync(b->dctrl, b->hctrl, b->n * sizeof(CtrlState), cudaMemcpyHostToDevice, b->stream));
   }
-  SGNB_BCU(b, cudaStreamSynchronize(b->stream));
-  SGNB_BCU(b, cudaMemcpy(b->hctrl, b->dctrl, b->n * sizeof(CtrlState), cudaMemcpyDeviceToHost));
+  long long a1 = 0;
+  for (int i = 0; i < b->n; ++i) a1 = std::max(a1, b->hctrl[i].attempts);
+  b->launches = 1 + 4 * (a1 - a0);
   for (int i = 0; i < b->n; ++i) b->ctx[i]->cur = b->hctrl[i].cur;
   return SGNB_OK;
 }
@@ -1248,6 +1270,8 @@ int sgnb_batch_create(const sgnb_desc* descs, int n, sgnb_batch** out) {
   if (e == cudaSuccess) e = cudaMalloc(&b->dargsM, n * sizeof(StageArgsM));
   if (e == cudaSuccess) e = cudaMallocHost(&b->hargsM, n * sizeof(StageArgsM));
   if (e == cudaSuccess) e = cudaMalloc(&b->dctrl, n * sizeof(CtrlState));
+  if (e == cudaSuccess) e = cudaMalloc(&b->dcount, 2 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->dcount, 0, 2 * sizeof(int));
   if (e == cudaSuccess) e = cudaMallocHost(&b->hctrl, n * sizeof(CtrlState));
   if (e == cudaSuccess) e = cudaMalloc(&b->dpart, n * sizeof(double*));
   if (e == cudaSuccess) e = cudaMalloc(&b->dntot, n * sizeof(long long));
@@ -1309,6 +1333,7 @@ int sgnb_batch_destroy(sgnb_batch* b) {
   if (b->chunk) cudaGraphExecDestroy(b->chunk);
   if (b->evRead) cudaEventDestroy(b->evRead);
   cudaFree(b->dconsts); cudaFree(b->dargs); cudaFree(b->dctrl); cudaFree(b->dpart);
+  cudaFree(b->dcount);
   cudaFree(b->dntot); cudaFree(b->dpartbuf);
   if (b->hargs) cudaFreeHost(b->hargs);
   cudaFree(b->dargsM);

@@ -234,6 +234,13 @@ size_t fused_smem_bytes();
 // the attempt count has reached attemptCap.
 cudaError_t launch_controller_loop(CtrlState* c, const double* partials, int nblk, long long n,
                                    cudaGraphConditionalHandle loop, cudaStream_t s);
+// Batched form of the loop controller: block i runs instance i's controller; every block
+// counts whether its instance still runs, and the last block to finish (an atomic ticket,
+// no waiting) sets the condition (any instance running) and clears the two counters.
+cudaError_t launch_controller_batch_loop(CtrlState* ctrls, const double* const* partials,
+                                         const int* nblk, const long long* n, int ninst,
+                                         int* counters, cudaGraphConditionalHandle loop,
+                                         cudaStream_t s);
 cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk,
                               long long n, cudaStream_t s);
 // Largest eta = h - H inside a window, with its node: (value, index) per block.

@@ -123,6 +123,23 @@ __global__ void __launch_bounds__(kCtrlThreads) k_controller_loop(CtrlState* c, 
     cudaGraphSetConditional(loop, (c->done == 0 && c->attempts < c->attemptCap) ? 1u : 0u);
 }
 
+__global__ void __launch_bounds__(kCtrlThreads) k_controller_batch_loop(
+    CtrlState* ctrls, const double* const* partials, const int* nblk, const long long* n,
+    int* counters, cudaGraphConditionalHandle loop) {
+  const int i = blockIdx.x;
+  CtrlState* c = ctrls + i;
+  controller_block(c, partials[i], nblk[i], n[i]);
+  if (threadIdx.x != 0) return;
+  if (c->done == 0 && c->attempts < c->attemptCap) atomicAdd(&counters[0], 1);
+  __threadfence();
+  if (atomicAdd(&counters[1], 1) == (int)gridDim.x - 1) {  // the last block of this attempt
+    __threadfence();
+    const int running = atomicExch(&counters[0], 0);
+    counters[1] = 0;
+    cudaGraphSetConditional(loop, running > 0 ? 1u : 0u);
+  }
+}
+
 // Slab controller: the error blocks of every slab of a decomposed mesh, read in place (on
 // other devices: peer loads) in slab order, as one list.
 __global__ void __launch_bounds__(kCtrlThreads) k_controller_slabs(CtrlState* c, const SlabPartials L,
@@ -199,6 +216,14 @@ cudaError_t launch_controller(CtrlState* c, const double* partials, int nblk, lo
 cudaError_t launch_controller_loop(CtrlState* c, const double* partials, int nblk, long long n,
                                    cudaGraphConditionalHandle loop, cudaStream_t s) {
   k_controller_loop<<<1, kCtrlThreads, 0, s>>>(c, partials, nblk, n, loop);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_controller_batch_loop(CtrlState* ctrls, const double* const* partials,
+                                         const int* nblk, const long long* n, int ninst,
+                                         int* counters, cudaGraphConditionalHandle loop,
+                                         cudaStream_t s) {
+  k_controller_batch_loop<<<ninst, kCtrlThreads, 0, s>>>(ctrls, partials, nblk, n, counters, loop);
   return cudaGetLastError();
 }
 
