@@ -250,8 +250,14 @@ int build_loop_graph(sgnb_ctx* c) {
 // controller state between launches.
 int run_loop(sgnb_ctx* c) {
   constexpr long long kAttemptsPerLaunch = 4096;
-  int rc = build_loop_graph(c);
-  if (rc) return rc;
+  // SGNB_HOST_LOOP=1: the same kernels launched from the host, 16 attempts between reads of
+  // the controller (kernel-replay profilers do not see kernels inside conditional nodes)
+  const char* hl = std::getenv("SGNB_HOST_LOOP");
+  const bool host_loop = hl && hl[0] == '1';
+  if (!host_loop) {
+    int rc = build_loop_graph(c);
+    if (rc) return rc;
+  }
   CtrlState& h = *c->hctrl;
   h.attemptCap = h.attempts + kAttemptsPerLaunch;
   SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
@@ -261,15 +267,26 @@ int run_loop(sgnb_ctx* c) {
   // FSAL head: k1 = R(u) into K1[cur] (FP32 in the mixed mode)
   SGNB_CU(c, launch(c, rhs_launch(c->U[c->cur], c->mixed ? nullptr : (double*)c->K1[c->cur]),
                     c->stream));
+  long long host_attempts = 0;  // attempts launched by the host loop (finished runs' exit at entry)
   for (;;) {
-    SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
+    if (host_loop) {
+      host_attempts += 16;
+      for (int k = 0; k < 16; ++k) {
+        SGNB_CU(c, launch(c, stage_launch(2), c->stream));
+        SGNB_CU(c, launch(c, stage_launch(3), c->stream));
+        SGNB_CU(c, launch(c, stage_launch(4), c->stream));
+        SGNB_CU(c, dev::launch_controller(c->dctrl, c->partials, c->nblk, c->ntot, c->stream));
+      }
+    } else {
+      SGNB_CU(c, cudaGraphLaunch(c->chunk, c->stream));
+    }
     SGNB_CU(c, cudaMemcpyAsync(c->hctrl, c->dctrl, sizeof(CtrlState), cudaMemcpyDeviceToHost, c->stream));
     SGNB_CU(c, cudaStreamSynchronize(c->stream));
     if (h.done) break;
     h.attemptCap = h.attempts + kAttemptsPerLaunch;  // more attempts than one launch allows
     SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, c->stream));
   }
-  c->launches = per_rhs + per_attempt * (h.attempts - attempts0);
+  c->launches = per_rhs + per_attempt * (host_loop ? host_attempts : h.attempts - attempts0);
   c->cur = h.cur;
   return SGNB_OK;
 }
