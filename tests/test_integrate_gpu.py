@@ -154,3 +154,28 @@ def test_zero_length_interval():
         st = d.integrate_adaptive(0.5, 0.5, 1e-3)
         assert (st.accepted, st.rejected, st.rhsEvals) == (0, 0, 1)
         assert bits_equal(d.download(), U)
+
+
+def test_device_loop_matches_host_loop_and_relaunches(monkeypatch):
+    """The device-side loop (a CUDA-graph WHILE node whose controller sets the condition)
+    and the host-launched loop (SGNB_HOST_LOOP=1) run the same kernels: bit for bit the
+    same run. 5000 steps cross the device loop's 4096-attempt bound on one graph launch,
+    so the host relaunches it once; launch counts are exact on the device loop."""
+    kw, U = bump_case(1, Nx=4, Ny=3, Lx=5.0, Ly=4.0)
+    runs = {}
+    for mode in ("device", "host"):
+        if mode == "host":
+            monkeypatch.setenv("SGNB_HOST_LOOP", "1")
+        else:
+            monkeypatch.delenv("SGNB_HOST_LOOP", raising=False)
+        with sgnb.SGN2DB200(precision=sgnb.FP64_EXACT, **kw) as d:
+            d.upload(U)
+            dt0 = d.cfl_time_step(0.5)
+            st = d.integrate_steps(0.0, dt0, 5000)
+            runs[mode] = (d.download(), st)
+    (ud, sd), (uh, sh) = runs["device"], runs["host"]
+    assert (sd.accepted, sd.rejected, sd.attempts) == (sh.accepted, sh.rejected, sh.attempts)
+    assert sd.accepted == 5000 and sd.attempts > 4096
+    assert bits_equal(ud, uh) and sd.tReached == sh.tReached
+    assert sd.kernel_launches == 1 + 4 * sd.attempts
+    assert sh.kernel_launches >= sd.kernel_launches
