@@ -222,6 +222,12 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
  * tests can compare them with the IEEE results. */
 int sgnb_fast_math(int fn, const double* x, double* y, long long n, void* stream);
 
+/* The checked build (libsgnb_checked.so, compiled with -DSGNB_CHECKED) range-checks every
+ * global access of the fused FP64 kernels against its buffer; an out-of-range index is
+ * counted and the access skipped. The count on `device` since the last reset (reset != 0
+ * zeroes it after reading). SGNB_ERR_UNSUPPORTED in the normal build. */
+int sgnb_checked_oob(int device, long long* count, int reset);
+
 /* Slab decomposition (the reference's multi-GPU solver, src/cuda/sgn2d_cuda_mpi.cu:148-161,
  * 487-537: x slabs, one halo exchange per right-hand side, one reduction of the error norm
  * per step). A slab is a context created with Nx_global / ex_offset; its neighbours'

@@ -947,6 +947,23 @@ int batch_run(sgnb_batch* b) {
 
 extern "C" {
 
+int sgnb_checked_oob(int device, long long* count, int reset) {
+  if (!count) return fail(nullptr, SGNB_ERR_INVALID, "count is NULL");
+  *count = 0;
+#ifdef SGNB_CHECKED
+  cudaError_t e = cudaSetDevice(device);
+  unsigned long long a = 0, b = 0;
+  if (e == cudaSuccess) e = dev::read_oob_exact(&a, reset != 0);
+  if (e == cudaSuccess) e = dev::read_oob_fast(&b, reset != 0);
+  if (e != cudaSuccess) return fail(nullptr, SGNB_ERR_CUDA, cudaGetErrorString(e));
+  *count = (long long)(a + b);
+  return SGNB_OK;
+#else
+  (void)device; (void)reset;
+  return fail(nullptr, SGNB_ERR_UNSUPPORTED, "not the checked build (libsgnb_checked.so)");
+#endif
+}
+
 int sgnb_fast_math(int fn, const double* x, double* y, long long n, void* stream) {
   if ((fn != 0 && fn != 1) || n < 0 || (n > 0 && (!x || !y)))
     return fail(nullptr, SGNB_ERR_INVALID, "fn 0 or 1, device arrays x, y of n doubles");

@@ -11,6 +11,23 @@ cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A, 
 }
 cudaError_t prepare_fused_fast() { return prepare_all(); }
 
+// The checked build's out-of-range count of this translation unit's kernels (reset: then
+// zero it); cudaErrorNotSupported in the normal build.
+cudaError_t read_oob_fast(unsigned long long* out, bool reset) {
+#ifdef SGNB_CHECKED
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_sgnb_oob, sizeof(*out));
+  if (e == cudaSuccess && reset) {
+    const unsigned long long z = 0;
+    e = cudaMemcpyToSymbol(g_sgnb_oob, &z, sizeof(z));
+  }
+  return e;
+#else
+  *out = 0;
+  (void)reset;
+  return cudaErrorNotSupported;
+#endif
+}
+
 // The fast mode's reciprocal (fn 0) and square root (fn 1) on a device array, for tests.
 __global__ void k_fast_math(int fn, const double* __restrict__ x, double* __restrict__ y,
                             long long n) {

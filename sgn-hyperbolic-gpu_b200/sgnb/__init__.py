@@ -24,7 +24,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsgnb.so")
+# SGNB_LIBRARY=checked selects the range-checked build libsgnb_checked.so (tests)
+LIB_PATH = os.path.join(HERE, "libsgnb_checked.so" if os.environ.get("SGNB_LIBRARY") == "checked"
+                        else "libsgnb.so")
 
 BC_PERIODIC = 0
 BC_WALL = 1
@@ -145,6 +147,7 @@ SIGNATURES = {
     "sgnb_fr_tables_points": (C.c_int, [C.c_int, C.c_int] + [_dp] * 7),
     "sgnb_setup_bathymetry": (C.c_int, [C.POINTER(_Desc)] + [_dp] * 7),
     "sgnb_fast_math": (C.c_int, [C.c_int, _dp, _dp, C.c_longlong, C.c_void_p]),
+    "sgnb_checked_oob": (C.c_int, [C.c_int, C.POINTER(C.c_longlong), C.c_int]),
     "sgnb_set_ghosts": (C.c_int, [C.c_void_p, _dp, _dp]),
     "sgnb_slab_pack": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_void_p]),
     "sgnb_slab_begin": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,

@@ -1,0 +1,86 @@
+"""Runs every fused FP64 kernel family of the range-checked build (libsgnb_checked.so) on
+ragged meshes and prints the out-of-range access count as the last line ("oob N").
+
+Started by tests/test_checked_gpu.py in its own process with SGNB_LIBRARY=checked, so that
+this process loads the checked library instead of the normal one. Covers the right-hand
+side and the BS3(2) stages (exact and fast modes, periodic and walls, partial tiles, Manning
+friction), Gauss-Legendre points (trace pre-pass and GAUSS variant), the batched kernels in
+every tile shape and grid form, and slab edges (ghost reads, fused edge writes, packs).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "sgn-hyperbolic-gpu_b200"))
+sys.path.insert(0, HERE)
+
+import sgnb  # noqa: E402
+from cases import bump_case, gauss_case  # noqa: E402
+from sgnb.slabs import PeerSlabSolver, SlabSolver  # noqa: E402
+
+MESHES = [(2, 2), (3, 2), (8, 6), (9, 5), (17, 3), (13, 11)]
+
+
+def count(reset=False):
+    n = C.c_longlong()
+    rc = sgnb.lib().sgnb_checked_oob(0, C.byref(n), int(reset))
+    if rc != 0:
+        raise SystemExit("not the checked build")
+    return n.value
+
+
+def main():
+    assert os.path.basename(sgnb.LIB_PATH) == "libsgnb_checked.so", sgnb.LIB_PATH
+    count(reset=True)
+    for Nx, Ny in MESHES:
+        for bc in (0, 1):
+            kw, U = bump_case(bc, Nx=Nx, Ny=Ny, Lx=1.25 * Nx, Ly=1.3 * Ny)
+            for prec in (sgnb.FP64_EXACT, sgnb.FP64_FAST):
+                for n_man in (0.0, 0.03):
+                    with sgnb.SGN2DB200(precision=prec, **dict(kw, nManning=n_man)) as d:
+                        d.rhs(U)
+                        d.upload(U)
+                        d.integrate_steps(0.0, d.cfl_time_step(0.4), 3)
+            gk, GU = gauss_case(bc, Nx=Nx, Ny=Ny, Lx=1.25 * Nx, Ly=1.3 * Ny)
+            with sgnb.SGN2DB200(precision=sgnb.FP64_FAST, **gk) as d:
+                d.rhs(GU)
+                d.upload(GU)
+                d.integrate_steps(0.0, d.cfl_time_step(0.4), 2)
+    # batches: every tile shape, one CTA per tile and persistent grids
+    insts = []
+    for i, (Nx, Ny) in enumerate(MESHES):
+        kw, _ = bump_case(i % 2, Nx=Nx, Ny=Ny, Lx=1.25 * Nx, Ly=1.3 * Ny)
+        kw = dict(kw)
+        kw.pop("P")
+        insts.append(kw)
+    b = sgnb.SGNBatch(insts)
+    for shape in (0, 1, 2):
+        for blocks in (0, 148):
+            for i, kw in enumerate(insts):
+                _, U = bump_case(i % 2, Nx=kw["Nx"], Ny=kw["Ny"], Lx=kw["Lx"], Ly=kw["Ly"])
+                b[i].upload(U)
+            b.config = (shape, blocks)
+            b.integrate_steps(np.full(len(insts), 1e-3), 2)
+    b.close()
+    # slabs: ghost reads, packs, fused edge writes, controllers on all slabs' partials
+    for bc in (0, 1):
+        kw, U = bump_case(bc, Nx=13, Ny=5, Lx=6.5, Ly=4.0)
+        kw = dict(kw, precision=sgnb.FP64_FAST)
+        with SlabSolver(kw, nslabs=3) as s:
+            s.rhs(U)
+            s.upload(U)
+            s.integrate_steps(0.0, 1e-3, 3)
+        with PeerSlabSolver(kw, nslabs=3, streams="per-slab") as s:
+            s.rhs(U)
+            s.upload(U)
+            s.integrate_steps(0.0, 1e-3, 3)
+    print(f"oob {count()}")
+
+
+if __name__ == "__main__":
+    main()
