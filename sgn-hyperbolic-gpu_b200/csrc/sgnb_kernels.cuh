@@ -101,10 +101,10 @@ struct Tile {
 #define SGNB_FAST_MIN_CTAS 2
 #endif
 
-// Index checks of the checked build (-DSGNB_CHECKED, libsgnb_checked.so): inb(i, n) is
+// Index checks of the checked build (-DSGNB_CHECKED, libsgnb_checked.so): SGNB_INB(i, n) is
 // false, and the out-of-range access is counted (g_sgnb_oob, one counter per translation
-// unit) and skipped, when i is outside [0, n). In the normal build it is the constant true
-// and the checks compile away.
+// unit) and skipped, when i is outside [0, n). In the normal build it is the literal true,
+// so the kernels compile exactly as without the checks.
 #ifdef SGNB_CHECKED
 static __device__ unsigned long long g_sgnb_oob;
 __device__ __forceinline__ bool inb(long long i, long long n) {
@@ -112,8 +112,9 @@ __device__ __forceinline__ bool inb(long long i, long long n) {
   atomicAdd(&g_sgnb_oob, 1ULL);
   return false;
 }
+#define SGNB_INB(i, n) inb((i), (n))
 #else
-__device__ __forceinline__ constexpr bool inb(long long, long long) { return true; }
+#define SGNB_INB(i, n) true
 #endif
 
 // Asynchronous global -> shared copy of one double (cp.async, no register staging), and
@@ -520,7 +521,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
-        if (inb(gof[u], Nd) && inb(sof[u], TE * NPP)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+        if (SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
       }
     if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) {
       const double* __restrict__ src = MODE == MODE_RHS ? I.in : I.u;
@@ -528,7 +529,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u] && inb(gof[u], Nd) && inb(sof[u], TE * NPP)) {
+          if (okk[u] && SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) {
             cp_async8(&(&S.U[v][0][0])[sof[u]], src + (long long)v * Nd + gof[u]);
             if constexpr (MODE == MODE_STAGE)
               cp_async8(&(&S.G[v][0][0])[sof[u]], I.k + (long long)v * Nd + gof[u]);
@@ -539,7 +540,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u] && inb(gof[u], Nd) && inb(sof[u], TE * NPP)) {
+          if (okk[u] && SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) {
             cp_async8(&(&S.U[v][0][0])[sof[u]], I.k1 + (long long)v * Nd + gof[u]);
             cp_async8(&(&S.G[v][0][0])[sof[u]], I.k2 + (long long)v * Nd + gof[u]);
           }
@@ -592,12 +593,12 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NHIT; ++u)
       if (hq[u] >= 0) {
         if constexpr (GAUSS)
-          hv[u] = inb(hg[u], 4 * Nd) ? C.tr[hg[u]] : 0.0;
+          hv[u] = SGNB_INB(hg[u], 4 * Nd) ? C.tr[hg[u]] : 0.0;
         else if constexpr (GHOST)
-          hv[u] = hs[u] == 0 ? (inb(hg[u], NV * Nd) ? stage_value<MODE>(I, hg[u]) : 0.0)
-                             : (inb(hg[u], (long long)NV * Ny * NP) ? (hs[u] == 1 ? C.ghostL : C.ghostR)[hg[u]] : 0.0);
+          hv[u] = hs[u] == 0 ? (SGNB_INB(hg[u], NV * Nd) ? stage_value<MODE>(I, hg[u]) : 0.0)
+                             : (SGNB_INB(hg[u], (long long)NV * Ny * NP) ? (hs[u] == 1 ? C.ghostL : C.ghostR)[hg[u]] : 0.0);
         else
-          hv[u] = inb(hg[u], NV * Nd) ? stage_value<MODE>(I, hg[u]) : 0.0;
+          hv[u] = SGNB_INB(hg[u], NV * Nd) ? stage_value<MODE>(I, hg[u]) : 0.0;
       }
     // face depths
     double fv[NFIT];
@@ -611,7 +612,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
         const int ix = i % TX, iy = i / TX;
         if (ix < TXv && iy < TYv) {
           const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
-          fv[u] = inb(e * NP + t, Nd / NP) ? (s == 0 ? C.HfX : C.HfY)[e * NP + t] : 0.0;
+          fv[u] = SGNB_INB(e * NP + t, Nd / NP) ? (s == 0 ? C.HfX : C.HfY)[e * NP + t] : 0.0;
           fq[u] = q;
         }
       } else if (q < NFACE) {
@@ -620,27 +621,38 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
         if (slot < TY) {
           if (slot < TYv) {
             const int ey = ey0 + slot;
-            const long long fe = (wallR || ghostR) ? (long long)ey * NP + t
-                                 : ((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t;
-            fv[u] = inb(fe, (wallR || ghostR) ? (long long)Ny * NP : Nd / NP)
-                        ? ((wallR || ghostR) ? C.HfXEnd : C.HfX)[fe] : 0.0;
+#ifdef SGNB_CHECKED
+            const long long fe = (long long)ey * NP + t;
+            const long long fx = ((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t;
+            fv[u] = (wallR || ghostR) ? (SGNB_INB(fe, (long long)Ny * NP) ? C.HfXEnd[fe] : 0.0)
+                                      : (SGNB_INB(fx, Nd / NP) ? C.HfX[fx] : 0.0);
+#else
+            fv[u] = (wallR || ghostR) ? C.HfXEnd[(long long)ey * NP + t]
+                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
+#endif
             fq[u] = q;
           }
         } else if (slot - TY < TXv) {
           const int ex = ex0 + slot - TY;
-          const long long fe = wallT ? (long long)ex * NP + t
-                                     : ((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t;
-          fv[u] = inb(fe, wallT ? (long long)Nx * NP : Nd / NP) ? (wallT ? C.HfYEnd : C.HfY)[fe] : 0.0;
+#ifdef SGNB_CHECKED
+          const long long fe = (long long)ex * NP + t;
+          const long long fy = ((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t;
+          fv[u] = wallT ? (SGNB_INB(fe, (long long)Nx * NP) ? C.HfYEnd[fe] : 0.0)
+                        : (SGNB_INB(fy, Nd / NP) ? C.HfY[fy] : 0.0);
+#else
+          fv[u] = wallT ? C.HfYEnd[(long long)ex * NP + t]
+                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t];
+#endif
           fq[u] = q;
         }
       }
     }
 #pragma unroll
     for (int u = 0; u < NHIT; ++u)
-      if (hq[u] >= 0 && inb(hq[u], NV * NHALO * NP)) S.halo[hq[u]] = hv[u];
+      if (hq[u] >= 0 && SGNB_INB(hq[u], NV * NHALO * NP)) S.halo[hq[u]] = hv[u];
 #pragma unroll
     for (int u = 0; u < NFIT; ++u)
-      if (fq[u] >= 0 && inb(fq[u], NFACE)) S.Hf[fq[u]] = fv[u];
+      if (fq[u] >= 0 && SGNB_INB(fq[u], NFACE)) S.Hf[fq[u]] = fv[u];
     cp_async_wait_all();
     if constexpr (MODE == MODE_STAGE) {
       // u + (c dt) k for this thread's own items (rk.cpp:100-103), in shared memory
@@ -663,7 +675,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u] && inb(gof[u], Nd)) ux[v][u] = I.u[(long long)v * Nd + gof[u]];
+          if (okk[u] && SGNB_INB(gof[u], Nd)) ux[v][u] = I.u[(long long)v * Nd + gof[u]];
 #pragma unroll
       for (int v = 0; v < NV; ++v)
 #pragma unroll
@@ -671,7 +683,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
           if (okk[u]) {
             double& y = (&S.U[v][0][0])[sof[u]];
             y = fsal_part(y, (&S.G[v][0][0])[sof[u]]);
-            if (inb(gof[u], Nd) && inb(sof[u], TE * NPP))
+            if (SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP))
               cp_async8(&(&S.G[v][0][0])[sof[u]], I.k3 + (long long)v * Nd + gof[u]);
           }
       double* __restrict__ unew = A.U[cur ^ 1];
@@ -684,7 +696,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             double& y = (&S.U[v][0][0])[sof[u]];
             const double un = fsal_finish(ux[v][u], y, (&S.G[v][0][0])[sof[u]], I.dt);
             y = un;
-            if (inb(gof[u], Nd)) unew[(long long)v * Nd + gof[u]] = un;
+            if (SGNB_INB(gof[u], Nd)) unew[(long long)v * Nd + gof[u]] = un;
           }
       }
     }
@@ -856,7 +868,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u] && inb(gof[u], Nd)) outp[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
+          if (okk[u] && SGNB_INB(gof[u], Nd)) outp[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
     } else {
       // One field at a time, with the next field's four arrays prefetched while the
       // current field's error is formed: hoisting every field's loads at once would
@@ -867,7 +879,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           const long long g = gof[u];
-          if (inb(g, Nd)) { uu[u] = I.u[g]; c1[u] = I.k1[g]; c2[u] = I.k2[g]; c3[u] = I.k3[g]; }
+          if (SGNB_INB(g, Nd)) { uu[u] = I.u[g]; c1[u] = I.k1[g]; c2[u] = I.k2[g]; c3[u] = I.k3[g]; }
         }
 #pragma unroll 1
       for (int v = 0; v < NV; ++v) {
@@ -876,14 +888,14 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
           for (int u = 0; u < NIT; ++u)
             if (okk[u]) {
               const long long g = (long long)(v + 1) * Nd + gof[u];
-              if (inb(g, NV * Nd)) { nu[u] = I.u[g]; n1[u] = I.k1[g]; n2[u] = I.k2[g]; n3[u] = I.k3[g]; }
+              if (SGNB_INB(g, NV * Nd)) { nu[u] = I.u[g]; n1[u] = I.k1[g]; n2[u] = I.k2[g]; n3[u] = I.k3[g]; }
             }
         }
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
             const double k4 = (&S.G[v][0][0])[sof[u]];
-            if (inb(gof[u], Nd)) outp[(long long)v * Nd + gof[u]] = k4;
+            if (SGNB_INB(gof[u], Nd)) outp[(long long)v * Nd + gof[u]] = k4;
             // scaled embedded error, src/solver/rk.cpp:118-128; the candidate uNew is
             // still in the tile (the passes only read S.U)
             const double dt = I.dt;
@@ -939,7 +951,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
         const long long g = (long long)v * Nd + ((long long)(ex0 + ixe) + (long long)Nx * (ey0 + iy)) * NPP + node;
         const double kout = S.G[v][TX * iy + ixe][node];
         const long long ge = (long long)v * Ny * NP + (long long)(ey0 + iy) * NP + t;
-        if (!inb(g, NV * Nd) || !inb(ge, (long long)NV * Ny * NP)) continue;
+        if (!SGNB_INB(g, NV * Nd) || !SGNB_INB(ge, (long long)NV * Ny * NP)) continue;
         const double val = A.kin_k2 == 0 ? stage_axpy(u0[g], 0.75 * dt, kout)
                                           : fsal_finish(u0[g], fsal_part(k1[g], k2[g]), kout, dt);
         (side == 0 ? C.edgeL : C.edgeR)[ge] = val;
@@ -1027,8 +1039,8 @@ __global__ void __launch_bounds__(256) k_traces(const RhsConsts C, const StageAr
       line[k] = stage_value<MODE>(I, (long long)v * C.Nd + e * NPP + (dir == 0 ? k + NP * t : t + NP * k));
     const long long lo = ((long long)(fl * NV + v) * ne + e) * NP + t;
     const long long hi = ((long long)((fl + 1) * NV + v) * ne + e) * NP + t;
-    if (inb(lo, 100 * ne)) C.tr[lo] = face_trace(C.lL, line, 1);
-    if (inb(hi, 100 * ne)) C.tr[hi] = face_trace(C.lR, line, 1);
+    if (SGNB_INB(lo, 100 * ne)) C.tr[lo] = face_trace(C.lL, line, 1);
+    if (SGNB_INB(hi, 100 * ne)) C.tr[hi] = face_trace(C.lR, line, 1);
   }
 }
 
