@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include "sgnb_device.h"
+#include "sgnb_checked.cuh"
 #include "sgnb_fastmath.cuh"
 
 namespace sgnb {
@@ -99,22 +100,6 @@ struct Tile {
 // register budget per thread follows: 2 -> 168 registers, 3 -> 128).
 #ifndef SGNB_FAST_MIN_CTAS
 #define SGNB_FAST_MIN_CTAS 2
-#endif
-
-// Index checks of the checked build (-DSGNB_CHECKED, libsgnb_checked.so): SGNB_INB(i, n) is
-// false, and the out-of-range access is counted (g_sgnb_oob, one counter per translation
-// unit) and skipped, when i is outside [0, n). In the normal build it is the literal true,
-// so the kernels compile exactly as without the checks.
-#ifdef SGNB_CHECKED
-static __device__ unsigned long long g_sgnb_oob;
-__device__ __forceinline__ bool inb(long long i, long long n) {
-  if (i >= 0 && i < n) return true;
-  atomicAdd(&g_sgnb_oob, 1ULL);
-  return false;
-}
-#define SGNB_INB(i, n) inb((i), (n))
-#else
-#define SGNB_INB(i, n) true
 #endif
 
 // Asynchronous global -> shared copy of one double (cp.async, no register staging), and

@@ -13,6 +13,23 @@ static cudaError_t launch_m(const RhsConsts& C, const StageArgsM& A, cudaStream_
   return cudaGetLastError();
 }
 
+// The checked build's out-of-range count of the mixed kernels (reset: then zero it);
+// cudaErrorNotSupported in the normal build.
+cudaError_t read_oob_mixed(unsigned long long* out, bool reset) {
+#ifdef SGNB_CHECKED
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_sgnb_oob, sizeof(*out));
+  if (e == cudaSuccess && reset) {
+    const unsigned long long z = 0;
+    e = cudaMemcpyToSymbol(g_sgnb_oob, &z, sizeof(z));
+  }
+  return e;
+#else
+  *out = 0;
+  (void)reset;
+  return cudaErrorNotSupported;
+#endif
+}
+
 cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
   switch (mode) {
     case 0: return launch_m<mix::MODE_RHS>(C, A, s);

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include "sgnb_device.h"
+#include "sgnb_checked.cuh"
 #include "sgnb_fastmath.cuh"
 
 namespace sgnb {
@@ -291,7 +292,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
-        cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+        if (SGNB_INB(gof[u], Nd)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
       }
     double* __restrict__ unew = A.U[cur ^ 1];
     if constexpr (MODE == MODE_STAGE) {
@@ -300,7 +301,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u]) {
+          if (okk[u] && SGNB_INB(gof[u], Nd)) {
             const unsigned sa = (unsigned)__cvta_generic_to_shared(&(&S.G[v][0][0])[sof[u]]);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
                          "l"(I.k + (long long)v * Nd + gof[u]) : "memory");
@@ -319,7 +320,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
         for (int v = 0; v < NV; ++v)
 #pragma unroll
           for (int u = 0; u < NIT; ++u)
-            if (okk[u]) {
+            if (okk[u] && SGNB_INB(gof[u], Nd)) {
               const unsigned sa = (unsigned)__cvta_generic_to_shared(k12_slot(w, v) + sof[u]);
               asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
                            "l"((w == 0 ? I.k1 : I.k2) + (long long)v * Nd + gof[u]) : "memory");
@@ -334,7 +335,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u]) {
+          if (okk[u] && SGNB_INB(gof[u], Nd)) {
             ux[v][u] = I.u[(long long)v * Nd + gof[u]];
             if constexpr (MODE == MODE_FSAL) k3x[v][u] = I.k3[(long long)v * Nd + gof[u]];
           }
@@ -352,14 +353,15 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
             x[u] = fsal_m(ux[v][u], k12_slot(0, v)[sof[u]], k12_slot(1, v)[sof[u]], k3x[v][u],
                           I.dt);
           else
-            x[u] = stage_value<MODE>(I, (long long)v * Nd + gof[u]);
+            x[u] = SGNB_INB(gof[u], Nd) ? stage_value<MODE>(I, (long long)v * Nd + gof[u]) : 0.0;
         }
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           if (v == 0) (&S.h[0][0])[sof[u]] = x[u];
           else (&S.q[v - 1][0][0])[sof[u]] = (float)x[u];
-          if constexpr (MODE == MODE_FSAL) unew[(long long)v * Nd + gof[u]] = x[u];
+          if constexpr (MODE == MODE_FSAL)
+            if (SGNB_INB(gof[u], Nd)) unew[(long long)v * Nd + gof[u]] = x[u];
         }
     }
     // halos
@@ -396,7 +398,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     }
 #pragma unroll
     for (int u = 0; u < NHIT; ++u)
-      if (hq[u] >= 0) hv[u] = stage_value<MODE>(I, hg[u]);
+      if (hq[u] >= 0 && SGNB_INB(hg[u], NV * Nd)) hv[u] = stage_value<MODE>(I, hg[u]);
     double fv[NFIT];
     int fq[NFIT];
 #pragma unroll
@@ -408,7 +410,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
         const int ix = i % TX, iy = i / TX;
         if (ix < TXv && iy < TYv) {
           const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
-          fv[u] = (s == 0 ? C.HfX : C.HfY)[e * NP + t];
+          fv[u] = SGNB_INB(e * NP + t, Nd / NP) ? (s == 0 ? C.HfX : C.HfY)[e * NP + t] : 0.0;
           fq[u] = q;
         }
       } else if (q < NFACE) {
@@ -417,21 +419,29 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
         if (slot < TY) {
           if (slot < TYv) {
             const int ey = ey0 + slot;
-            fv[u] = wallR ? C.HfXEnd[(long long)ey * NP + t]
-                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
+            fv[u] = SGNB_INB(wallR ? (long long)ey * NP + t
+                                   : ((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t,
+                             wallR ? (long long)Ny * NP : Nd / NP)
+                        ? (wallR ? C.HfXEnd[(long long)ey * NP + t]
+                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t])
+                        : 0.0;
             fq[u] = q;
           }
         } else if (slot - TY < TXv) {
           const int ex = ex0 + slot - TY;
-          fv[u] = wallT ? C.HfYEnd[(long long)ex * NP + t]
-                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t];
+          fv[u] = SGNB_INB(wallT ? (long long)ex * NP + t
+                                 : ((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t,
+                           wallT ? (long long)Nx * NP : Nd / NP)
+                      ? (wallT ? C.HfYEnd[(long long)ex * NP + t]
+                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t])
+                      : 0.0;
           fq[u] = q;
         }
       }
     }
 #pragma unroll
     for (int u = 0; u < NHIT; ++u)
-      if (hq[u] >= 0) {
+      if (hq[u] >= 0 && SGNB_INB(hq[u], NV * NHALO * NP)) {
         const int q = hq[u];
         const int v = q / (NHALO * NP), rest = q - v * NHALO * NP;
         if (v == 0) S.hhalo[rest] = hv[u];
@@ -439,7 +449,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       }
 #pragma unroll
     for (int u = 0; u < NFIT; ++u)
-      if (fq[u] >= 0) S.Hf[fq[u]] = fv[u];
+      if (fq[u] >= 0 && SGNB_INB(fq[u], NFACE)) S.Hf[fq[u]] = fv[u];
     cp_async_wait_all();
   }
   __syncthreads();
@@ -577,7 +587,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
-        if (okk[u]) {
+        if (okk[u] && SGNB_INB(gof[u], Nd)) {
           const float val = (&S.G[v][0][0])[sof[u]];
           if (A.outd) A.outd[(long long)v * Nd + gof[u]] = (double)val;
           else A.out[(long long)v * Nd + gof[u]] = val;
@@ -587,7 +597,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
-        if (okk[u]) A.out[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
+        if (okk[u] && SGNB_INB(gof[u], Nd)) A.out[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
   } else {
     const volatile CtrlState* vc = A.ctrl;
     cur = vc->cur;
@@ -606,7 +616,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
         const long long g = gof[u];
-        uu[u] = u0[g]; c1[u] = k1p[g]; c2[u] = k2p[g]; c3[u] = k3p[g];
+        if (SGNB_INB(g, Nd)) { uu[u] = u0[g]; c1[u] = k1p[g]; c2[u] = k2p[g]; c3[u] = k3p[g]; }
       }
 #pragma unroll 1
     for (int v = 0; v < NV; ++v) {
@@ -615,14 +625,14 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
             const long long g = (long long)(v + 1) * Nd + gof[u];
-            nu[u] = u0[g]; n1[u] = k1p[g]; n2[u] = k2p[g]; n3[u] = k3p[g];
+            if (SGNB_INB(g, NV * Nd)) { nu[u] = u0[g]; n1[u] = k1p[g]; n2[u] = k2p[g]; n3[u] = k3p[g]; }
           }
       }
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           const float k4 = (&S.G[v][0][0])[sof[u]];
-          outp[(long long)v * Nd + gof[u]] = k4;
+          if (SGNB_INB(gof[u], Nd)) outp[(long long)v * Nd + gof[u]] = k4;
           const double b1 = c1[u], b2 = c2[u], b3 = c3[u], b4 = k4;
           const double un = uu[u] + dt * (2.0 / 9.0 * b1 + 1.0 / 3.0 * b2 + 4.0 / 9.0 * b3);
           const double uEmb = uu[u] + dt * (7.0 / 24.0 * b1 + 0.25 * b2 + 1.0 / 3.0 * b3 + 0.125 * b4);

@@ -3,9 +3,9 @@ ragged meshes and prints the out-of-range access count as the last line ("oob N"
 
 Started by tests/test_checked_gpu.py in its own process with SGNB_LIBRARY=checked, so that
 this process loads the checked library instead of the normal one. Covers the right-hand
-side and the BS3(2) stages (exact and fast modes, periodic and walls, partial tiles, Manning
-friction), Gauss-Legendre points (trace pre-pass and GAUSS variant), the batched kernels in
-every tile shape and grid form, and slab edges (ghost reads, fused edge writes, packs).
+side and the BS3(2) stages (exact, fast and mixed modes, periodic and walls, partial tiles,
+Manning friction), Gauss-Legendre points (trace pre-pass and GAUSS variant), the batched kernels in
+every tile shape and grid form (mixed batches too), and slab edges (ghost reads, fused edge writes, packs).
 """
 from __future__ import annotations
 
@@ -40,7 +40,7 @@ def main():
     for Nx, Ny in MESHES:
         for bc in (0, 1):
             kw, U = bump_case(bc, Nx=Nx, Ny=Ny, Lx=1.25 * Nx, Ly=1.3 * Ny)
-            for prec in (sgnb.FP64_EXACT, sgnb.FP64_FAST):
+            for prec in (sgnb.FP64_EXACT, sgnb.FP64_FAST, sgnb.MIXED):
                 for n_man in (0.0, 0.03):
                     with sgnb.SGN2DB200(precision=prec, **dict(kw, nManning=n_man)) as d:
                         d.rhs(U)
@@ -67,6 +67,14 @@ def main():
             b.config = (shape, blocks)
             b.integrate_steps(np.full(len(insts), 1e-3), 2)
     b.close()
+    bm = sgnb.SGNBatch(insts, precision=sgnb.MIXED)
+    for blocks in (0, 148):
+        for i, kw in enumerate(insts):
+            _, U = bump_case(i % 2, Nx=kw["Nx"], Ny=kw["Ny"], Lx=kw["Lx"], Ly=kw["Ly"])
+            bm[i].upload(U)
+        bm.config = (0, blocks)
+        bm.integrate_steps(np.full(len(insts), 1e-3), 2)
+    bm.close()
     # slabs: ghost reads, packs, fused edge writes, controllers on all slabs' partials
     for bc in (0, 1):
         kw, U = bump_case(bc, Nx=13, Ny=5, Lx=6.5, Ly=4.0)

@@ -1,5 +1,5 @@
 """The range-checked build (libsgnb_checked.so, -DSGNB_CHECKED): every global access of the
-fused FP64 kernels is checked against its buffer and an out-of-range index is counted and
+fused FP64 and mixed-precision kernels is checked against its buffer and an out-of-range index is counted and
 skipped instead of performed. tests/checked_run.py drives every kernel family on ragged
 meshes in its own process (SGNB_LIBRARY=checked selects the library); the count must be
 zero. The normal build answers SGNB_ERR_UNSUPPORTED to the count query."""
