@@ -223,7 +223,8 @@ int sgnb_setup_bathymetry(const sgnb_desc* d, double* Hnod, double* Hx, double* 
 int sgnb_fast_math(int fn, const double* x, double* y, long long n, void* stream);
 
 /* The checked build (libsgnb_checked.so, compiled with -DSGNB_CHECKED) range-checks every
- * global access of the fused FP64 and mixed-precision kernels against its buffer; an out-of-range index is
+ * global access of the fused FP64 and mixed-precision kernels and of the adjoint's
+ * kernels against its buffer; an out-of-range index is
  * counted and the access skipped. The count on `device` since the last reset (reset != 0
  * zeroes it after reading). SGNB_ERR_UNSUPPORTED in the normal build. */
 int sgnb_checked_oob(int device, long long* count, int reset);

@@ -22,6 +22,7 @@
 // The gather kernel (one thread per node) sums the two directions and the neighbours'
 // face contributions in a fixed order, so the result is deterministic without atomics,
 // and folds in the RK-stage combination. Built with -fmad=true like the fast forward.
+#include "sgnb_checked.cuh"
 #include "sgnb_device.h"
 
 namespace sgnb {
@@ -124,12 +125,13 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
     const long long g = node(m);
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-      L.U[m][v] = stage_in(A, v * Nd + g);
-      double r = A.alpha * A.ra[v * Nd + g];
-      if (A.rb) r += A.beta * A.rb[v * Nd + g];
+      const bool ok = SGNB_INB(v * Nd + g, NV * Nd);
+      L.U[m][v] = ok ? stage_in(A, v * Nd + g) : 0.0;
+      double r = ok ? A.alpha * A.ra[v * Nd + g] : 0.0;
+      if (A.rb && ok) r += A.beta * A.rb[v * Nd + g];
       Rb[m][v] = r;
     }
-    L.H[m] = C.Hnod[g];
+    L.H[m] = SGNB_INB(g, Nd) ? C.Hnod[g] : 0.0;
   }
   bool wallLo, wallHi;
   long long nLo, nHi;  // neighbour trace nodes
@@ -141,8 +143,9 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
     const long long eR = (long long)((ex + 1) % C.Nx) + (long long)C.Nx * ey;
     nLo = eL * NPP + (NP - 1) + NP * j;
     nHi = eR * NPP + NP * j;
-    HfLo = C.HfX[e * NP + j];
-    HfHi = wallHi ? C.HfXEnd[(long long)ey * NP + j] : C.HfX[eR * NP + j];
+    HfLo = SGNB_INB(e * NP + j, ne * NP) ? C.HfX[e * NP + j] : 0.0;
+    HfHi = SGNB_INB(wallHi ? (long long)ey * NP + j : eR * NP + j, wallHi ? (long long)C.Ny * NP : ne * NP)
+               ? (wallHi ? C.HfXEnd[(long long)ey * NP + j] : C.HfX[eR * NP + j]) : 0.0;
   } else {
     wallLo = C.bcy && ey == 0;
     wallHi = C.bcy && ey == C.Ny - 1;
@@ -150,14 +153,17 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
     const long long eT = (long long)ex + (long long)C.Nx * ((ey + 1) % C.Ny);
     nLo = eB * NPP + j + NP * (NP - 1);
     nHi = eT * NPP + j;
-    HfLo = C.HfY[e * NP + j];
-    HfHi = wallHi ? C.HfYEnd[(long long)ex * NP + j] : C.HfY[eT * NP + j];
+    HfLo = SGNB_INB(e * NP + j, ne * NP) ? C.HfY[e * NP + j] : 0.0;
+    HfHi = SGNB_INB(wallHi ? (long long)ex * NP + j : eT * NP + j, wallHi ? (long long)C.Nx * NP : ne * NP)
+               ? (wallHi ? C.HfYEnd[(long long)ex * NP + j] : C.HfY[eT * NP + j]) : 0.0;
   }
   double sLo[NV], sHi[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    sLo[v] = wallLo ? (v == nd ? -L.U[0][v] : L.U[0][v]) : stage_in(A, v * Nd + nLo);
-    sHi[v] = wallHi ? (v == nd ? -L.U[NP - 1][v] : L.U[NP - 1][v]) : stage_in(A, v * Nd + nHi);
+    sLo[v] = wallLo ? (v == nd ? -L.U[0][v] : L.U[0][v])
+                    : (SGNB_INB(v * Nd + nLo, NV * Nd) ? stage_in(A, v * Nd + nLo) : 0.0);
+    sHi[v] = wallHi ? (v == nd ? -L.U[NP - 1][v] : L.U[NP - 1][v])
+                    : (SGNB_INB(v * Nd + nHi, NV * Nd) ? stage_in(A, v * Nd + nHi) : 0.0);
   }
   const double* tLo = L.U[0];
   const double* tHi = L.U[NP - 1];
@@ -284,6 +290,7 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
     for (int m = 0; m < NP; ++m) {
       const long long g = node(m);
       const double* U = L.U[m];
+      if (!SGNB_INB(g, Nd)) continue;
       const double Hx = C.Hx[g], Hy = C.Hy[g];
       const double ih = 1.0 / U[0];
       const double u = U[1] * ih, v = U[2] * ih, p = U[4] * ih;
@@ -320,7 +327,8 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
   } else {
     double* o = A.Sn[DIR][0] + idx * NV;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) o[v] = sLb[v];
+    for (int v = 0; v < NV; ++v)
+      if (SGNB_INB(idx * NV + v, ne * NP * NV)) o[v] = sLb[v];
   }
   if (wallHi) {
 #pragma unroll
@@ -328,13 +336,17 @@ __global__ void __launch_bounds__(128) k_vjp_lines(const RhsConsts C, const FrTa
   } else {
     double* o = A.Sn[DIR][1] + idx * NV;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) o[v] = sHb[v];
+    for (int v = 0; v < NV; ++v)
+      if (SGNB_INB(idx * NV + v, ne * NP * NV)) o[v] = sHb[v];
   }
-  A.Hf[DIR][0][idx] = HfLb;
-  A.Hf[DIR][1][idx] = HfHb;
+  if (SGNB_INB(idx, ne * NP)) {
+    A.Hf[DIR][0][idx] = HfLb;
+    A.Hf[DIR][1][idx] = HfHb;
+  }
 #pragma unroll
   for (int m = 0; m < NP; ++m) {
     const long long g = node(m);
+    if (!SGNB_INB(g, Nd)) continue;
 #pragma unroll
     for (int v = 0; v < NV; ++v) A.Ub[DIR][v * Nd + g] = Ub[m][v];
     A.Hb[DIR][g] = Hb[m];
@@ -363,10 +375,11 @@ __global__ void __launch_bounds__(256) k_vjp_gather(const RhsConsts C, const Vjp
     const long long g = v * Nd + gnode;
     double y = A.Ub[0][g] + A.Ub[1][g];
     // line index of a face entry: (element * 5 + line) * 5 + v
-    if (a == 0 && !wL) y += A.Sn[0][1][(eL * NP + b) * NV + v];
-    if (a == NP - 1 && !wR) y += A.Sn[0][0][(eR * NP + b) * NV + v];
-    if (b == 0 && !wB) y += A.Sn[1][1][(eB * NP + a) * NV + v];
-    if (b == NP - 1 && !wT) y += A.Sn[1][0][(eT * NP + a) * NV + v];
+    [[maybe_unused]] const long long nl = (long long)C.Nx * C.Ny * NP * NV;
+    if (a == 0 && !wL && SGNB_INB((eL * NP + b) * NV + v, nl)) y += A.Sn[0][1][(eL * NP + b) * NV + v];
+    if (a == NP - 1 && !wR && SGNB_INB((eR * NP + b) * NV + v, nl)) y += A.Sn[0][0][(eR * NP + b) * NV + v];
+    if (b == 0 && !wB && SGNB_INB((eB * NP + a) * NV + v, nl)) y += A.Sn[1][1][(eB * NP + a) * NV + v];
+    if (b == NP - 1 && !wT && SGNB_INB((eT * NP + a) * NV + v, nl)) y += A.Sn[1][0][(eT * NP + a) * NV + v];
     if (G.ybar) G.ybar[g] = y;
     if (G.init) G.uacc[g] = (G.lam ? G.lam[g] : 0.0) + y;
     else G.uacc[g] += y;
@@ -374,18 +387,23 @@ __global__ void __launch_bounds__(256) k_vjp_gather(const RhsConsts C, const Vjp
   G.Hacc[gnode] += A.Hb[0][gnode] + A.Hb[1][gnode];
   G.Hxacc[gnode] += A.Hxb[gnode];
   G.Hyacc[gnode] += A.Hyb[gnode];
-  if (a == 0) {
+  [[maybe_unused]] const long long nf = (long long)C.Nx * C.Ny * NP;
+  if (a == 0 && SGNB_INB(e * NP + b, nf) && SGNB_INB(eL * NP + b, nf)) {
     double s = A.Hf[0][0][e * NP + b];
     if (!wL) s += A.Hf[0][1][eL * NP + b];
     G.HfXacc[e * NP + b] += s;
   }
-  if (a == NP - 1 && wR) G.HfXEndacc[(long long)ey * NP + b] += A.Hf[0][1][e * NP + b];
-  if (b == 0) {
+  if (a == NP - 1 && wR && SGNB_INB((long long)ey * NP + b, (long long)C.Ny * NP) &&
+      SGNB_INB(e * NP + b, nf))
+    G.HfXEndacc[(long long)ey * NP + b] += A.Hf[0][1][e * NP + b];
+  if (b == 0 && SGNB_INB(e * NP + a, nf) && SGNB_INB(eB * NP + a, nf)) {
     double s = A.Hf[1][0][e * NP + a];
     if (!wB) s += A.Hf[1][1][eB * NP + a];
     G.HfYacc[e * NP + a] += s;
   }
-  if (b == NP - 1 && wT) G.HfYEndacc[(long long)ex * NP + a] += A.Hf[1][1][e * NP + a];
+  if (b == NP - 1 && wT && SGNB_INB((long long)ex * NP + a, (long long)C.Nx * NP) &&
+      SGNB_INB(e * NP + a, nf))
+    G.HfYEndacc[(long long)ex * NP + a] += A.Hf[1][1][e * NP + a];
 }
 
 // u_new = u + dt ((2/9 k1 + 1/3 k2) + 4/9 k3) with the end-point stage's rounding
@@ -406,7 +424,7 @@ __global__ void k_rk_update(const double* __restrict__ u, const double* __restri
 __global__ void k_gauges(const double* __restrict__ U, const double* __restrict__ Hnod,
                          const long long* __restrict__ nodes, int ng, double* __restrict__ eta) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < ng) eta[g] = U[nodes[g]] - Hnod[nodes[g]];
+  if (g < ng) eta[g] = U[nodes[g]] - Hnod[nodes[g]];  // nodes checked on the host
 }
 
 // lam[h](node_g) += etab[g]
@@ -418,6 +436,23 @@ __global__ void k_gauges_back(double* __restrict__ lam, const long long* __restr
 }
 
 }  // namespace
+
+// The checked build's out-of-range count of the adjoint kernels (reset: then zero it);
+// cudaErrorNotSupported in the normal build.
+cudaError_t read_oob_adjoint(unsigned long long* out, bool reset) {
+#ifdef SGNB_CHECKED
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_sgnb_oob, sizeof(*out));
+  if (e == cudaSuccess && reset) {
+    const unsigned long long z = 0;
+    e = cudaMemcpyToSymbol(g_sgnb_oob, &z, sizeof(z));
+  }
+  return e;
+#else
+  *out = 0;
+  (void)reset;
+  return cudaErrorNotSupported;
+#endif
+}
 
 cudaError_t launch_vjp_rhs(const RhsConsts& C, const FrTablesDev& T, const VjpArgs& A,
                            const GatherArgs& G, cudaStream_t s) {

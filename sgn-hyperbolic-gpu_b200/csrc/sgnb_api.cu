@@ -952,12 +952,13 @@ int sgnb_checked_oob(int device, long long* count, int reset) {
   *count = 0;
 #ifdef SGNB_CHECKED
   cudaError_t e = cudaSetDevice(device);
-  unsigned long long a = 0, b = 0, m = 0;
+  unsigned long long a = 0, b = 0, m = 0, j = 0;
   if (e == cudaSuccess) e = dev::read_oob_exact(&a, reset != 0);
   if (e == cudaSuccess) e = dev::read_oob_fast(&b, reset != 0);
   if (e == cudaSuccess) e = dev::read_oob_mixed(&m, reset != 0);
+  if (e == cudaSuccess) e = dev::read_oob_adjoint(&j, reset != 0);
   if (e != cudaSuccess) return fail(nullptr, SGNB_ERR_CUDA, cudaGetErrorString(e));
-  *count = (long long)(a + b + m);
+  *count = (long long)(a + b + m + j);
   return SGNB_OK;
 #else
   (void)device; (void)reset;

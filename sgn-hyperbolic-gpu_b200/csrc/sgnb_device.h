@@ -178,6 +178,7 @@ cudaError_t prepare_mixed_batch();
 cudaError_t read_oob_exact(unsigned long long* out, bool reset);
 cudaError_t read_oob_fast(unsigned long long* out, bool reset);
 cudaError_t read_oob_mixed(unsigned long long* out, bool reset);
+cudaError_t read_oob_adjoint(unsigned long long* out, bool reset);
 
 // The fast mode's reciprocal (fn 0) and square root (fn 1) elementwise, for tests.
 cudaError_t launch_fast_math(int fn, const double* x, double* y, long long n, cudaStream_t s);
