@@ -28,7 +28,27 @@ __device__ __forceinline__ void controller_core(CtrlState* c, const Row& row, lo
   if (c->done) return;
   const int t = threadIdx.x;
   double s = 0.0, m = 0.0, nn = 0.0;
-  for (long long b = t; b < nblk; b += kCtrlThreads) {
+  // rows b = t, t + T, t + 2T, ... in this order; eight rows' loads are issued before
+  // they are summed, so the walk takes one memory latency per eight rows
+  constexpr int kAhead = 8;
+  long long b = t;
+  for (; b + (kAhead - 1) * kCtrlThreads < nblk; b += kAhead * kCtrlThreads) {
+    double r0[kAhead], r1[kAhead], r2[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) {
+      const double* r = row(b + k * kCtrlThreads);
+      r0[k] = r[0];
+      r1[k] = r[1];
+      r2[k] = r[2];
+    }
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) {
+      s += r0[k];
+      m = dmax(m, r1[k]);
+      nn += r2[k];
+    }
+  }
+  for (; b < nblk; b += kCtrlThreads) {
     const double* r = row(b);
     s += r[0];
     m = dmax(m, r[1]);
