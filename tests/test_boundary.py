@@ -106,6 +106,10 @@ def test_host_bathymetry_bitwise(kind, par, bc):
     (dict(precision=9), 2),
     (dict(bathy_kind=42), 1),
     (dict(bathy_kind=sgnb.BATHY_GAUSS, bathy_par=(1.0,)), 1),  # parameter vector too short
+    (dict(Ny=1), 1),            # SGN2D: Nx, Ny >= 2
+    (dict(Lx=0.0), 1),          # a degenerate domain (hx = Lx / Nx, mesh2d.h:27) is refused
+    (dict(Ly=-1.0), 1),
+    (dict(Nx=9269, Ny=9268), 1),  # 25 Nx Ny nodes per field must stay below 2^31
 ])
 def test_create_rejects_bad_arguments(kw, code):
     args = dict(Nx=8, Ny=6)
@@ -113,6 +117,19 @@ def test_create_rejects_bad_arguments(kw, code):
     with pytest.raises(sgnb.SgnbError) as ei:
         sgnb.SGN2DB200(**args)
     assert ei.value.status == code
+
+
+def test_largest_mesh_passes_validation():
+    """9268 x 9268 elements (25 Nx Ny = 2,147,395,600 nodes per field, just below 2^31) passes
+    argument validation and reaches the device check; one element column more is refused
+    above."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is visible (the mesh would be allocated)")
+    with pytest.raises(sgnb.SgnbError) as ei:
+        sgnb.SGN2DB200(Nx=9268, Ny=9268)
+    assert ei.value.status == 8
 
 
 def test_create_without_device_fails_loudly():
