@@ -157,6 +157,11 @@ int sgnb_integrate_steps(sgnb_ctx* ctx, double t0, double dt0, long long nsteps,
 /* n consecutive bs3Step (src/solver/rk.h:50) steps of the uploaded state with the
  * given step sizes, starting at t0: the frozen-dt replay of an accepted sequence. */
 int sgnb_bs3_steps(sgnb_ctx* ctx, double t0, const double* dts, long long n);
+/* n consecutive rk4Step (src/solver/rk.h:42, classical RK4, src/solver/rk.cpp:23-38) steps
+ * of the uploaded state with the given step sizes, starting at t0 (the right-hand side
+ * does not depend on t). FP64 modes; SGNB_ERR_UNSUPPORTED in the mixed mode. Like the
+ * reference it checks nothing: a non-finite state stays in the buffer. */
+int sgnb_rk4_steps(sgnb_ctx* ctx, double t0, const double* dts, long long n);
 
 /* Attempt log of the last sgnb_integrate_adaptive / sgnb_bs3_steps call: per attempt
  * (t, dt, errNorm, accepted as 1.0 / 0.0), up to 65536 attempts. Copies min(cap, n)

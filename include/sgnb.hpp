@@ -157,6 +157,10 @@ class SGN2DB200 {
   void bs3Steps(double t0, const std::vector<double>& dts) {
     check(sgnb_bs3_steps(ctx_, t0, dts.data(), (long long)dts.size()), ctx_);
   }
+  // Consecutive rk4Step calls with given step sizes (classical RK4; FP64 modes).
+  void rk4Steps(double t0, const std::vector<double>& dts) {
+    check(sgnb_rk4_steps(ctx_, t0, dts.data(), (long long)dts.size()), ctx_);
+  }
 
   double mass() { return scalar(&sgnb_mass); }
   double energy() { return scalar(&sgnb_energy); }

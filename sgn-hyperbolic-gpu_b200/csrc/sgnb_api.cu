@@ -659,6 +659,67 @@ int sgnb_bs3_steps(sgnb_ctx* c, double t0, const double* dts, long long n) {
   return SGNB_OK;
 }
 
+// rk4Step (src/solver/rk.cpp:23-38) per given step size: k1 = R(u) into K1[cur], then the
+// fused stage kernel three times with the stage coefficient 1/2 (k1 -> K2), 1/2 (K2 -> K3)
+// and 1 (K3 -> K1[cur ^ 1]): its u + (c dt) k rounds as u + 0.5 * dt * k and u + dt * k
+// do on the CPU (c dt is exact for c = 1/2 and 1). The update writes the state in place.
+int sgnb_rk4_steps(sgnb_ctx* c, double t0, const double* dts, long long n) {
+  (void)t0;  // R does not depend on t
+  if (!c || (n > 0 && !dts) || n < 0) return fail(c, SGNB_ERR_INVALID, "bad arguments");
+  if (c->C.ghostL || c->C.ghostR)
+    return fail(c, SGNB_ERR_INVALID, "a slab integrates through the slab entries (sgnb_slab_*)");
+  if (c->mixed) return fail(c, SGNB_ERR_UNSUPPORTED, "rk4 steps run in the FP64 modes");
+  if (n == 0) return SGNB_OK;
+  if (int rc = set_device(c)) return rc;
+  if (n > c->dtCap) {
+    cudaFree(c->dtList);
+    c->dtList = nullptr;
+    SGNB_CU(c, cudaMalloc(&c->dtList, n * sizeof(double)));
+    c->dtCap = n;
+  }
+  SGNB_CU(c, cudaMemcpy(c->dtList, dts, n * sizeof(double), cudaMemcpyHostToDevice));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  CtrlState& h = *c->hctrl;
+  sgnb_rk_opts o;
+  sgnb_rk_opts_init(&o);
+  init_ctrl(c, h, o);  // done = 0: the stage kernels run
+  h.cur = c->cur;
+  h.log = nullptr;
+  cudaStream_t s = c->stream;
+  SGNB_CU(c, cudaMemcpyAsync(c->dctrl, c->hctrl, sizeof(CtrlState), cudaMemcpyHostToDevice, s));
+  const int cur = c->cur;
+  double* u = c->U[cur];
+  double* k1 = (double*)c->K1[cur];
+  double* k2 = (double*)c->K2;
+  double* k3 = (double*)c->K3;
+  double* k4 = (double*)c->K1[cur ^ 1];
+  auto stage = [&](const double* kin, double coef, double* out) {
+    StageArgs A{};
+    A.U[0] = c->U[0]; A.U[1] = c->U[1];
+    A.K1[0] = (double*)c->K1[0]; A.K1[1] = (double*)c->K1[1];
+    A.K2 = const_cast<double*>(kin);  // the stage kernel adds A.K2 when kin_k2 is set
+    A.K3 = k3;
+    A.kin_k2 = 1;
+    A.coef = coef;
+    A.out = out;
+    A.ctrl = c->dctrl;
+    A.partials = c->partials;
+    return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(1, c->C, A, s)
+                                          : dev::launch_fused_exact(1, c->C, A, s);
+  };
+  for (long long i = 0; i < n; ++i) {
+    SGNB_CU(c, dev::launch_rk4_set_dt(c->dctrl, c->dtList, i, s));
+    SGNB_CU(c, launch(c, rhs_launch(u, k1), s));  // k1 = R(u)
+    SGNB_CU(c, stage(k1, 0.5, k2));                // k2 = R(u + 0.5 dt k1)
+    SGNB_CU(c, stage(k2, 0.5, k3));                // k3 = R(u + 0.5 dt k2)
+    SGNB_CU(c, stage(k3, 1.0, k4));                // k4 = R(u + dt k3)
+    SGNB_CU(c, dev::launch_rk4_update(u, k1, k2, k3, k4, c->dctrl, c->ntot, sms, s));
+  }
+  SGNB_CU(c, cudaStreamSynchronize(s));
+  return SGNB_OK;
+}
+
 static int diag(sgnb_ctx* c, int what, double* out) {
   if (!c || !out) return fail(c, SGNB_ERR_INVALID, "NULL argument");
   if (int rc = set_device(c)) return rc;

@@ -231,6 +231,11 @@ int batch_tile_tx(int shape_id);
 cudaError_t launch_controller_batch(CtrlState* ctrls, const double* const* partials,
                                     const int* nblk, const long long* n, int ninst,
                                     cudaStream_t s);
+// rk4Step: c->dt = dts[i], and the final update u += dt/6 (k1 + 2 k2 + 2 k3 + k4) over n values
+cudaError_t launch_rk4_set_dt(CtrlState* c, const double* dts, long long i, cudaStream_t s);
+cudaError_t launch_rk4_update(double* u, const double* k1, const double* k2, const double* k3,
+                              const double* k4, const CtrlState* c, long long n, int sms,
+                              cudaStream_t s);
 size_t fused_smem_bytes();
 
 // Controller of one adaptive attempt: deterministic reduction of the per-CTA error

@@ -260,6 +260,40 @@ cudaError_t launch_controller_batch(CtrlState* ctrls, const double* const* parti
   return cudaGetLastError();
 }
 
+// ---- rk4Step (src/solver/rk.cpp:23-38) -------------------------------------------------
+// The three intermediate stages run the fused stage kernel, which reads the step size from
+// the controller state; this sets it for step i of a given list.
+__global__ void k_rk4_set_dt(CtrlState* c, const double* dts, long long i) { c->dt = dts[i]; }
+
+// u += (dt / 6) * (k1 + 2 k2 + 2 k3 + k4), summed left to right and every operation rounded
+// on its own, as the CPU evaluates rk.cpp:36-37 (this file is built with -fmad=false).
+__global__ void __launch_bounds__(256) k_rk4_update(double* __restrict__ u,
+                                                    const double* __restrict__ k1,
+                                                    const double* __restrict__ k2,
+                                                    const double* __restrict__ k3,
+                                                    const double* __restrict__ k4,
+                                                    const CtrlState* c, long long n) {
+  const double w = c->dt / 6.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double s = ((k1[i] + 2.0 * k2[i]) + 2.0 * k3[i]) + k4[i];
+    u[i] = u[i] + w * s;
+  }
+}
+
+cudaError_t launch_rk4_set_dt(CtrlState* c, const double* dts, long long i, cudaStream_t s) {
+  k_rk4_set_dt<<<1, 1, 0, s>>>(c, dts, i);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rk4_update(double* u, const double* k1, const double* k2, const double* k3,
+                              const double* k4, const CtrlState* c, long long n, int sms,
+                              cudaStream_t s) {
+  const long long want = (n + 255) / 256, cap = 8LL * sms;  // 8 blocks of 256 per SM
+  k_rk4_update<<<(unsigned)(want < cap ? want : cap), 256, 0, s>>>(u, k1, k2, k3, k4, c, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_reduce_diag(int what, const RhsConsts& C, const double* U, const double* qw,
                                double* out_partials, int nblk, cudaStream_t s) {
   QW q;

@@ -131,6 +131,7 @@ SIGNATURES = {
     "sgnb_integrate_steps": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_longlong,
                                        C.POINTER(_Opts), C.POINTER(_Stats)]),
     "sgnb_bs3_steps": (C.c_int, [C.c_void_p, C.c_double, _dp, C.c_longlong]),
+    "sgnb_rk4_steps": (C.c_int, [C.c_void_p, C.c_double, _dp, C.c_longlong]),
     "sgnb_launch_stage": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_void_p]),
     "sgnb_attempt_log": (C.c_int, [C.c_void_p, _dp, C.c_longlong, C.POINTER(C.c_longlong)]),
     "sgnb_max_wave_speed": (C.c_int, [C.c_void_p, _dp]),
@@ -452,6 +453,12 @@ class SGN2DB200:
         """Consecutive bs3Step calls with the given step sizes (frozen-dt replay)."""
         d = np.ascontiguousarray(dts, dtype=np.float64)
         _check(lib().sgnb_bs3_steps(self._h, t0, _ptr(d), int(d.size)), self._h)
+
+    def rk4_steps(self, t0, dts):
+        """Consecutive rk4Step calls (classical RK4, rk.cpp:23-38) with the given step
+        sizes; FP64 modes."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        _check(lib().sgnb_rk4_steps(self._h, t0, _ptr(d), int(d.size)), self._h)
 
     def attempt_log(self, cap=1 << 16):
         """Rows (t, dt, errNorm, accepted) of the last integration's attempts."""

@@ -126,6 +126,34 @@ int main() {
       diff = std::fmax(diff, std::fabs(Rc[i] - Rg[i]));
     report(same, "Gauss points: device rhs == SGN2D::rhs bit for bit", diff);
   }
+  {  // 5. fixed steps: the reference's rk4Step and bs3Step over rhsFn() against the device's
+    const double dt = host.cflTimeStep(U, 0.5);
+    const std::vector<double> dts = {dt, 0.8 * dt, dt};
+    sgn::State U4 = U, U3 = U;
+    double t = 0.0;
+    for (double d : dts) {
+      sgn::rk4Step(host.rhsFn(), t, d, U4);
+      sgn::bs3Step(host.rhsFn(), t, d, U3);
+      t += d;
+    }
+    sgnb::SGN2DB200 dev(host);
+    sgn::State G4, G3;
+    dev.upload(U);
+    dev.rk4Steps(0.0, dts);
+    dev.download(G4);
+    dev.upload(U);
+    dev.bs3Steps(0.0, dts);
+    dev.download(G3);
+    auto maxdiff = [](const sgn::State& a, const sgn::State& b) {
+      double d = 0.0;
+      for (size_t i = 0; i < a.size() && i < b.size(); ++i) d = std::fmax(d, std::fabs(a[i] - b[i]));
+      return d;
+    };
+    report(G4.size() == U4.size() && std::memcmp(G4.data(), U4.data(), U4.size() * sizeof(double)) == 0,
+           "3 x rk4Step: device == reference bit for bit", maxdiff(G4, U4));
+    report(G3.size() == U3.size() && std::memcmp(G3.data(), U3.data(), U3.size() * sizeof(double)) == 0,
+           "3 x bs3Step: device == reference bit for bit", maxdiff(G3, U3));
+  }
   std::printf(failures ? "%d FAILED\n" : "ALL PASSED\n", failures);
   return failures ? 1 : 0;
 }

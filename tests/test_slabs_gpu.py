@@ -116,6 +116,8 @@ def test_slab_contexts_refuse_whole_mesh_entries():
             ctx.integrate_steps(0.0, 1e-3, 2)
         with pytest.raises(sgnb.SgnbError):
             ctx.bs3_steps(0.0, [1e-3])
+        with pytest.raises(sgnb.SgnbError):
+            ctx.rk4_steps(0.0, [1e-3])
         from sgnb.adjoint import SGNAdjoint
 
         with pytest.raises(sgnb.SgnbError):
