@@ -20,6 +20,7 @@
 // sgnb::Error carrying the status and the library's message instead.
 #pragma once
 
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -134,6 +135,14 @@ class SGN2DB200 {
     if ((long long)U.size() != (long long)nTotal()) throw Error(SGNB_ERR_INVALID, "rhs: size mismatch");
     dU.resize(nTotal());
     check(sgnb_rhs_host(ctx_, U.data(), dU.data()), ctx_);
+  }
+  // rhs() in the shape of the reference's RhsFn, void(double t, const State&, State&)
+  // (src/solver/rk.h:39), as SGN2D::rhsFn() offers it (src/solver/sgn2d.h:79-80): the
+  // reference's host integrators (rk4Step, bs3Step, integrateAdaptive) then run with the
+  // device right-hand side, each call copying the state in and the derivative out. t is
+  // ignored. The returned callable refers to this object.
+  std::function<void(double, const std::vector<double>&, std::vector<double>&)> rhsFn() {
+    return [this](double, const std::vector<double>& U, std::vector<double>& dU) { rhs(U, dU); };
   }
   // rhs() for device pointers on a CUDA stream (0 = the context stream).
   void rhsDevice(const double* U, double* dU, void* stream = nullptr) {

@@ -47,11 +47,14 @@ def main():
                         d.rhs(U)
                         d.upload(U)
                         d.integrate_steps(0.0, d.cfl_time_step(0.4), 3)
+                        if prec != sgnb.MIXED:
+                            d.rk4_steps(0.0, [d.cfl_time_step(0.4)] * 2)
             gk, GU = gauss_case(bc, Nx=Nx, Ny=Ny, Lx=1.25 * Nx, Ly=1.3 * Ny)
             with sgnb.SGN2DB200(precision=sgnb.FP64_FAST, **gk) as d:
                 d.rhs(GU)
                 d.upload(GU)
                 d.integrate_steps(0.0, d.cfl_time_step(0.4), 2)
+                d.rk4_steps(0.0, [d.cfl_time_step(0.4)])
     # batches: every tile shape, one CTA per tile and persistent grids
     insts = []
     for i, (Nx, Ny) in enumerate(MESHES):

@@ -10,7 +10,10 @@
 //   3. an adaptive run (tEnd 0.3, atol 1e-10, rtol 1e-8) takes the CPU's accepted /
 //      rejected steps, ends within 1e-10 relative of the CPU state and conserves mass;
 //   4. a host solver on Gauss-Legendre points (flat bottom): its tables reach the device
-//      through the same constructor, and the device rhs equals SGN2D::rhs bit for bit.
+//      through the same constructor, and the device rhs equals SGN2D::rhs bit for bit;
+//   5. three fixed steps: the device's rk4Steps / bs3Steps equal the reference's rk4Step /
+//      bs3Step over host.rhsFn() bit for bit, and the reference's rk4Step over the device
+//      right-hand side (dev.rhsFn()) equals it too.
 // Prints one line per check and exits non-zero on any failure.
 #include "sgnb.hpp"
 
@@ -153,6 +156,15 @@ int main() {
            "3 x rk4Step: device == reference bit for bit", maxdiff(G4, U4));
     report(G3.size() == U3.size() && std::memcmp(G3.data(), U3.data(), U3.size() * sizeof(double)) == 0,
            "3 x bs3Step: device == reference bit for bit", maxdiff(G3, U3));
+    // the reference's own rk4Step driving the device right-hand side through rhsFn()
+    sgn::State H4 = U;
+    t = 0.0;
+    for (double d : dts) {
+      sgn::rk4Step(dev.rhsFn(), t, d, H4);
+      t += d;
+    }
+    report(std::memcmp(H4.data(), U4.data(), U4.size() * sizeof(double)) == 0,
+           "rk4Step over dev.rhsFn() == over host.rhsFn()", maxdiff(H4, U4));
   }
   std::printf(failures ? "%d FAILED\n" : "ALL PASSED\n", failures);
   return failures ? 1 : 0;
