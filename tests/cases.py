@@ -152,3 +152,40 @@ def cfg3_lake_case():
               bc_x=BC_PERIODIC, bc_y=BC_PERIODIC, bathy_kind=BATHY_GAUSS_SUM,
               bathy_par=cfg3_bathymetry())
     return kw
+
+
+def random_case(seed):
+    """A seeded random case: mesh, boundaries, g, gamma, c, Manning, solution points,
+    bathymetry and a smooth random state. In a walled direction the reference (on the
+    mirror-doubled domain) sees the wall problem only for bathymetry symmetric across the
+    wall, so a bump there is centred on 0 or on L."""
+    import oracle as O  # node coordinates and the set-up's nodal depth
+
+    rng = np.random.default_rng(seed)
+    Nx, Ny = int(rng.integers(2, 10)), int(rng.integers(2, 10))
+    Lx, Ly = float(rng.uniform(0.5, 3.0) * Nx), float(rng.uniform(0.5, 3.0) * Ny)
+    bc_x, bc_y = int(rng.integers(0, 2)), int(rng.integers(0, 2))
+    g = float(rng.uniform(1.0, 20.0))
+    kw = dict(P=4, Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, g=g, gamma=float(rng.uniform(0.5, 3.0)),
+              c=float(rng.uniform(0.0, 3.0) * np.sqrt(g)), bc_x=bc_x, bc_y=bc_y,
+              nManning=0.0 if rng.random() < 0.5 else float(rng.uniform(0.005, 0.05)))
+    points = O.POINTS_GAUSS if rng.random() < 0.25 else O.POINTS_GLL
+    H0 = float(rng.uniform(0.5, 1.5))
+    kind = O.BATHY_NONE if points == O.POINTS_GAUSS else int(rng.integers(0, 3))
+    if kind == O.BATHY_CONST:
+        par = (H0,)
+    elif kind == O.BATHY_GAUSS:
+        xc = float(rng.choice([0.0, Lx])) if bc_x else float(rng.uniform(0, Lx))
+        yc = float(rng.choice([0.0, Ly])) if bc_y else float(rng.uniform(0, Ly))
+        par = (H0, float(rng.uniform(0.0, 0.5) * H0), xc, yc, float(rng.uniform(0.5, 3.0) * Lx))
+    else:
+        par = ()
+    kw.update(bathy_kind=kind, bathy_par=par, points=points)
+    o = O.Oracle(**kw)
+    x, y = o.node_coords()
+    H = o.bathymetry()["Hnod"] if kind != O.BATHY_NONE else np.ones_like(x)
+    def smooth(a):
+        kx, ky = rng.integers(1, 3, 2) * 2 * np.pi / np.array([Lx, Ly])
+        return a * np.sin(kx * x + rng.uniform(0, 6.3)) * np.cos(ky * y + rng.uniform(0, 6.3))
+    U = o.make_state(H + smooth(0.05 * H0), smooth(0.1), smooth(0.1), smooth(0.02), smooth(0.02))
+    return kw, U

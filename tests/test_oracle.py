@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from cases import bump_case, cfg1_case, gauss_case, CFG1_STEPS, lake_case
+from cases import bump_case, cfg1_case, gauss_case, random_case, CFG1_STEPS, lake_case
 from conftest import bits_equal
 
 
@@ -90,6 +90,24 @@ def test_bathymetry_kinds_vs_reference(need_reference):
         ba, bb = oracle_for(kw).bathymetry(), oracle_for(kw, True).bathymetry()
         for k in ba:
             assert bits_equal(ba[k], bb[k]), (kind, k)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_cases_vs_reference(need_reference, seed):
+    """Forty seeded random cases: the restatement's rhs equals the reference's bit for bit
+    (Gauss points with a wall: to round-off, see test_gauss_vs_reference), and where both
+    directions are periodic one bs3Step and one rk4Step also agree bit for bit."""
+    kw, U = random_case(seed)
+    a, b = oracle_for(kw), oracle_for(kw, reference=True)
+    R, Rref = a.rhs(U), b.rhs(U)
+    if kw["points"] == O.POINTS_GAUSS and (kw["bc_x"] or kw["bc_y"]):
+        assert np.abs(R - Rref).max() <= 1e-13 * np.abs(Rref).max()
+    else:
+        assert bits_equal(R, Rref), kw
+        if not (kw["bc_x"] or kw["bc_y"]):
+            dt = 0.2 * a.cfl_time_step(U, 0.5)
+            assert bits_equal(a.bs3_step(U, 0.0, dt), b.bs3_step(U, 0.0, dt))
+            assert bits_equal(a.rk4_step(U, 0.0, dt), b.rk4_step(U, 0.0, dt))
 
 
 # --------------------------------------------------------------------------- golden

@@ -1,0 +1,39 @@
+"""Forty seeded random cases through the device right-hand side.
+
+tests/cases.py random_case: meshes of 2..9 x 2..9 elements, each direction periodic or
+walled, random g, gamma, c and Manning coefficient, GLL or Gauss-Legendre points, flat,
+constant or Gaussian-bump bathymetry, a smooth random state. The oracle's rhs of the same
+cases is pinned to the reference's bit for bit (tests/test_oracle.py). Bars:
+* exact mode: bit for bit; with Manning friction to the last-bit rounding of the cube root
+  (1e-15 relative per field: the device's and the host's cbrt may round differently);
+* fast mode: 1e-13 relative per field (GLL), 2e-13 (Gauss-Legendre points, whose traces
+  combine five nodes);
+* mixed mode (GLL only): its FP32 bar, 2e-5.
+"""
+from __future__ import annotations
+
+import pytest
+
+import oracle as O
+import sgnb
+from cases import random_case
+from conftest import bits_equal, rel_per_field
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_case_rhs(seed):
+    kw, U = random_case(seed)
+    R = O.Oracle(**kw).rhs(U)
+    gauss = kw["points"] == O.POINTS_GAUSS
+    with sgnb.SGN2DB200(precision=sgnb.FP64_EXACT, **kw) as d:
+        if kw["nManning"] > 0.0:
+            assert rel_per_field(d.rhs(U), R) < 1e-15
+        else:
+            assert bits_equal(d.rhs(U), R)
+    with sgnb.SGN2DB200(precision=sgnb.FP64_FAST, **kw) as d:
+        assert rel_per_field(d.rhs(U), R) < (2e-13 if gauss else 1e-13)
+    if not gauss:
+        with sgnb.SGN2DB200(precision=sgnb.MIXED, **kw) as d:
+            assert rel_per_field(d.rhs(U), R) < 2e-5
