@@ -211,7 +211,8 @@ def lib() -> C.CDLL:
 def _ptr(a):
     if a is None:
         return None
-    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], "float64 C-contiguous expected"
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("float64 C-contiguous array expected")
     return a.ctypes.data_as(_dp)
 
 
@@ -364,7 +365,10 @@ class SGN2DB200:
         _check(lib().sgnb_upload(self._h, _ptr(U)), self._h)
 
     def download(self, out=None):
-        out = np.empty(self.n) if out is None else out
+        if out is None:
+            out = np.empty(self.n)
+        elif not (isinstance(out, np.ndarray) and out.size == self.n and out.flags["WRITEABLE"]):
+            raise ValueError("SGN2DB200.download: out must be a writable array of 5 * nDof doubles")
         _check(lib().sgnb_download(self._h, _ptr(out)), self._h)
         return out
 
@@ -472,6 +476,8 @@ class SGN2DB200:
         (dict with the keys of setup_bathymetry)."""
         U = np.ascontiguousarray(U, dtype=np.float64)
         Rbar = np.ascontiguousarray(Rbar, dtype=np.float64)
+        if U.size != self.n or Rbar.size != self.n:
+            raise ValueError("rhs_vjp: U and Rbar must hold 5 * nDof values")
         Ub = np.empty(self.n)
         Nd, nf = self.Nd, 5 * self.Nx * self.Ny
         bars = dict(Hnod=np.zeros(Nd), Hx=np.zeros(Nd), Hy=np.zeros(Nd), HfaceX=np.zeros(nf),

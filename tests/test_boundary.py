@@ -150,3 +150,16 @@ def test_cases_match_oracle_coordinates():
     x, y = node_coords(4, kw["Nx"], kw["Ny"], kw["Lx"], kw["Ly"], gll5())
     xo, yo = o.node_coords()
     assert np.abs(x - xo).max() < 1e-14 and np.abs(y - yo).max() < 1e-14
+
+
+def test_host_buffers_must_be_contiguous_float64():
+    """Every host array handed to the library goes through sgnb._ptr, which refuses other
+    dtypes and strided views (the library reads and writes plain double arrays)."""
+    import numpy as np
+
+    assert sgnb._ptr(None) is None
+    sgnb._ptr(np.zeros(4))
+    with pytest.raises(ValueError):
+        sgnb._ptr(np.zeros(4, dtype=np.float32))
+    with pytest.raises(ValueError):
+        sgnb._ptr(np.zeros(8)[::2])

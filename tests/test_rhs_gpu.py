@@ -217,3 +217,22 @@ def test_embedding_vs_reference_1d(need_reference, axis, prec):
     # every line is the same line
     lines = R2[(0, nd, 3, 4), :, :, 0, :] if axis == "x" else R2[(0, nd, 3, 4), :, :, :, 0]
     assert np.abs(lines - lines[:, :1] if axis == "x" else lines - lines[:, :, :1]).max() < 1e-12
+
+
+def test_host_buffer_sizes_checked():
+    """Host arrays of the wrong size are refused before the library touches them."""
+    kw, U = bump_case(0)
+    with device(kw, sgnb.FP64_FAST) as d:
+        d.upload(U)
+        with pytest.raises(ValueError):
+            d.upload(U[:-1])
+        with pytest.raises(ValueError):
+            d.download(np.empty(U.size - 1))
+        with pytest.raises(ValueError):
+            d.download(np.empty(U.size, dtype=np.float32))
+        with pytest.raises(ValueError):
+            d.rhs(U[:-1])
+        with pytest.raises(ValueError):
+            d.rhs_vjp(U, U[:-5])
+        out = np.empty(U.size)
+        assert d.download(out) is out and bits_equal(out, U)
