@@ -361,7 +361,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           if (v == 0) (&S.h[0][0])[sof[u]] = x[u];
           else (&S.q[v - 1][0][0])[sof[u]] = (float)x[u];
           if constexpr (MODE == MODE_FSAL)
-            if (SGNB_INB(gof[u], Nd)) unew[(long long)v * Nd + gof[u]] = x[u];
+            if (SGNB_INB(gof[u], Nd)) __stcs(&unew[(long long)v * Nd + gof[u]], x[u]);
         }
     }
     // halos
@@ -578,6 +578,8 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   __syncthreads();
 
   // ---- copy-out and the FP64 embedded error of the end-point stage ---------------
+  // Results are stored, and the end-point stage's last reads of u, k1, k2, k3 loaded,
+  // with the streaming (evict-first) hint, as in the FP64 kernels.
   double esum = 0.0, emax = 0.0;
   int enan = 0;
   item_map();
@@ -589,15 +591,15 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       for (int u = 0; u < NIT; ++u)
         if (okk[u] && SGNB_INB(gof[u], Nd)) {
           const float val = (&S.G[v][0][0])[sof[u]];
-          if (A.outd) A.outd[(long long)v * Nd + gof[u]] = (double)val;
-          else A.out[(long long)v * Nd + gof[u]] = val;
+          if (A.outd) __stcs(&A.outd[(long long)v * Nd + gof[u]], (double)val);
+          else __stcs(&A.out[(long long)v * Nd + gof[u]], val);
         }
   } else if constexpr (MODE == MODE_STAGE) {
 #pragma unroll 1
     for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
-        if (okk[u] && SGNB_INB(gof[u], Nd)) A.out[(long long)v * Nd + gof[u]] = (&S.G[v][0][0])[sof[u]];
+        if (okk[u] && SGNB_INB(gof[u], Nd)) __stcs(&A.out[(long long)v * Nd + gof[u]], (&S.G[v][0][0])[sof[u]]);
   } else {
     const volatile CtrlState* vc = A.ctrl;
     cur = vc->cur;
@@ -616,7 +618,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
         const long long g = gof[u];
-        if (SGNB_INB(g, Nd)) { uu[u] = u0[g]; c1[u] = k1p[g]; c2[u] = k2p[g]; c3[u] = k3p[g]; }
+        if (SGNB_INB(g, Nd)) { uu[u] = __ldcs(&u0[g]); c1[u] = __ldcs(&k1p[g]); c2[u] = __ldcs(&k2p[g]); c3[u] = __ldcs(&k3p[g]); }
       }
 #pragma unroll 1
     for (int v = 0; v < NV; ++v) {
@@ -625,14 +627,14 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
             const long long g = (long long)(v + 1) * Nd + gof[u];
-            if (SGNB_INB(g, NV * Nd)) { nu[u] = u0[g]; n1[u] = k1p[g]; n2[u] = k2p[g]; n3[u] = k3p[g]; }
+            if (SGNB_INB(g, NV * Nd)) { nu[u] = __ldcs(&u0[g]); n1[u] = __ldcs(&k1p[g]); n2[u] = __ldcs(&k2p[g]); n3[u] = __ldcs(&k3p[g]); }
           }
       }
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           const float k4 = (&S.G[v][0][0])[sof[u]];
-          if (SGNB_INB(gof[u], Nd)) outp[(long long)v * Nd + gof[u]] = k4;
+          if (SGNB_INB(gof[u], Nd)) __stcs(&outp[(long long)v * Nd + gof[u]], k4);
           const double b1 = c1[u], b2 = c2[u], b3 = c3[u], b4 = k4;
           const double un = uu[u] + dt * (2.0 / 9.0 * b1 + 1.0 / 3.0 * b2 + 4.0 / 9.0 * b3);
           const double uEmb = uu[u] + dt * (7.0 / 24.0 * b1 + 0.25 * b2 + 1.0 / 3.0 * b3 + 0.125 * b4);
