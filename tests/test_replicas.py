@@ -56,3 +56,31 @@ def test_single_process_passthrough():
     import bench
 
     assert bench.reduce_over_ranks([1.5, 2.5], [3.0, 4.0], None, "cpu") == ([1.5, 2.5], [3.0, 4.0])
+
+
+def test_bench_reads_its_denominators():
+    """The roofline's inputs: the committed per-DOF DRAM traffic of the three kernel modes
+    (profiles/traffic_per_dof.txt) and the HBM peak (MEASURED_PEAKS.json, else the stated
+    fallback of 6650 GB/s)."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    t = bench.traffic_per_dof()
+    assert set(t) >= {"rhs", "stage", "fsal"}
+    # measured DRAM bytes stay near the algorithmic 18.24 / 26.24 / 50.24 B/DOF
+    for k, alg in (("rhs", 18.24), ("stage", 26.24), ("fsal", 50.24)):
+        assert 0.8 * alg < t[k] < 1.2 * alg, (k, t[k])
+    peak, kind = bench.measured_peak_hbm()
+    assert kind in ("measured", "fallback") and peak > 1000.0
+
+
+def test_reference_arm_other_ranks_do_nothing(monkeypatch, capsys):
+    """Under torchrun only rank 0 runs the reference arm; the others exit without work."""
+    sys.path.insert(0, ROOT)
+    import argparse
+
+    import bench
+
+    monkeypatch.setenv("RANK", "1")
+    bench.run_reference(argparse.Namespace(ref_device="cpu", steps=1, warmup=3, gpus=2))
+    assert capsys.readouterr().out == ""
