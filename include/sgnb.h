@@ -194,9 +194,10 @@ int sgnb_energy(sgnb_ctx* ctx, double* out);
  * for the energy. The result is written to out_dev[0] (device) asynchronously on
  * `stream` (NULL = the legacy default stream) on the current device.
  * Limit: 25 Nx Ny <= 67,108,864 nodes per field, else SGNB_ERR_INVALID.
- * The first call on a device looks up the array's device address; make that first call
- * before any stream capture. All calls on a device share the array: calls that overlap
- * on the GPU race. */
+ * Every call looks the array's device address up on the current device (so a device
+ * reset between calls leaves nothing stale); the first call on a device also loads the
+ * library's device code there, so make that first call before any stream capture. All
+ * calls on a device share the array: calls that overlap on the GPU race. */
 int sgnb_diag_noalloc(int what, int Nx, int Ny, double Lx, double Ly, double g, double c,
                       double gamma, const double* U_dev, const double* Hnod_dev,
                       double* out_dev, void* stream);
@@ -308,7 +309,9 @@ int sgnb_write_vtk(sgnb_ctx* ctx, const char* path);
 /* Batched sweep (no reference counterpart; the reference runs one instance per
  * SGN2DCuda): n independent instances (their own mesh size, parameters, bathymetry and
  * state) advanced together, one launch per RK stage over all instances' tiles, each
- * instance with its own adaptive controller, attempts replayed as CUDA-graph chunks. All
+ * instance with its own adaptive controller; the attempts run as a device-side loop (a
+ * CUDA graph whose WHILE conditional node repeats one attempt of every still-running
+ * instance until all are done). All
  * instances of a batch run in one arithmetic mode: SGNB_FP64_FAST (tile shapes 8x4, 16x2,
  * 4x8) or SGNB_MIXED (8x4 tiles). Instance i is an ordinary context
  * (sgnb_batch_instance) for upload / download / diagnostics between runs. */

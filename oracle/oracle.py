@@ -46,10 +46,17 @@ _libs: dict[str, C.CDLL] = {}
 _dp = C.POINTER(C.c_double)
 
 
+def reference_dir() -> str:
+    """The reference project's source tree: SGN_REFERENCE_DIR, else the checkout beside
+    this repository (the directory holding the repository's own directory)."""
+    return os.environ.get("SGN_REFERENCE_DIR",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+
+
 def build() -> None:
     """Compile liboracle.so (and _ref/libsgnref.so when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    ref = os.environ.get("SGN_REFERENCE_DIR", "/root/reference")
+    ref = reference_dir()
     if os.path.isdir(os.path.join(ref, "src", "solver")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 

@@ -3,10 +3,11 @@
 // The context owns the device state of one solver: the bathymetry statics, the state
 // ping-pong pair U[2], the FSAL pair K1[2] (k1 / k4), the stage derivatives K2, K3,
 // the per-CTA error partials and the device-resident controller state. An adaptive
-// integration is a sequence of graph launches, each replaying a chunk of attempts
-// (stage 2, stage 3, end-point stage, controller); the host reads the controller back
-// once per chunk instead of once per step (the reference copies error partials to the
-// host every step, src/cuda/sgn2d_cuda.cu:506-516).
+// integration is a device-side loop: a CUDA graph whose WHILE conditional node repeats one
+// attempt (stage 2, stage 3, end-point stage, controller) until the controller clears the
+// condition; the host reads the controller back once per graph launch instead of once per
+// step (the reference copies error partials to the host every step,
+// src/cuda/sgn2d_cuda.cu:506-516).
 #include "sgnb_ctx.h"
 
 #include <cmath>

@@ -92,6 +92,25 @@ def test_bathymetry_kinds_vs_reference(need_reference):
             assert bits_equal(ba[k], bb[k]), (kind, k)
 
 
+def test_cfg2_generator_vs_reference(need_reference):
+    """Configuration 2's own generator (the benchmark's: walls, elliptic shoal on the 0.45
+    plane, 8 seeded random-phase sines; sgnb.workloads) on a 256 x 128 mesh of the same
+    40 x 20 basin: the restatement's rhs, cfl step and one bs3Step equal the reference's
+    bit for bit. The reference sees the walls through mirror doubling; the shoal lies
+    inside [16, 24] x [7, 13], so the doubled domain's depth is the walled problem's."""
+    from sgnb import workloads as W
+
+    kw = W.cfg2_solver_args(256, 128)
+    U = W.cfg2_state_torch(256, 128, device="cpu").numpy()
+    a, b = oracle_for(kw), oracle_for(kw, reference=True)
+    R = a.rhs(U)
+    assert bits_equal(R, b.rhs(U))
+    assert np.abs(R).max() > 0
+    dt = a.cfl_time_step(U, 0.5)
+    assert dt == b.cfl_time_step(U, 0.5)
+    assert bits_equal(a.bs3_step(U, 0.0, dt), b.bs3_step(U, 0.0, dt))
+
+
 @pytest.mark.parametrize("seed", range(40))
 def test_random_cases_vs_reference(need_reference, seed):
     """Forty seeded random cases: the restatement's rhs equals the reference's bit for bit
