@@ -18,20 +18,23 @@
 // All calls on a device share the array. Each call writes every partial it reads before
 // reading it, so nothing has to be cleared between calls, but calls whose kernels overlap
 // on the GPU (different streams, no ordering between them) race on the partials.
+//
+// In host code the array's name is not a device address. Every call looks the address up
+// on the current device (cudaGetSymbolAddress, a host-side lookup that allocates nothing),
+// so no address outlives a device reset. The first call on a device also loads this
+// library's device code there; make that first call before any stream capture.
 #include "sgnb.h"
 #include "sgnb_setup.h"
 
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 
 namespace {
 
 constexpr int kDiagMaxBlocks = 16384;
 constexpr int kNodesPerBlock = 4096;
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) double g_diag_scratch[kDiagMaxBlocks];
 
@@ -39,10 +42,6 @@ struct DiagArgs {
   double g, c2, gamma;
   double qw[5];
 };
-
-// Device address of g_diag_scratch per device ordinal, looked up once per device.
-double* g_scratch_ptr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
 
 // Per-block partial over kNodesPerBlock consecutive nodes: what = 0 largest
 // characteristic speed (SGN2D::maxWaveSpeed, src/solver/sgn2d.cpp:295-305), 1 mass
@@ -56,10 +55,11 @@ __global__ void __launch_bounds__(kThreads) k_diag_partial(int what, DiagArgs a,
   for (int k = threadIdx.x; k < kNodesPerBlock; k += kThreads) {
     const long long i = base + k;
     if (i >= Nd) break;
-    const double h = U[i], hu = U[Nd + i], hv = U[2 * Nd + i];
+    const double h = U[i];
     const int loc = (int)(i % 25);
     const double wq = a.qw[loc % 5] * a.qw[loc / 5];
     if (what == 0) {
+      const double hu = U[Nd + i], hv = U[2 * Nd + i];
       const double p = U[4 * Nd + i] / h;
       const double arg = a.g * h + p + a.c2;
       const double ce = sqrt(arg > 0.0 ? arg : 0.0);
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(kThreads) k_diag_partial(int what, DiagArgs a,
     } else if (what == 1) {
       acc += wq * h;
     } else {
-      const double u = hu / h, v = hv / h, w = U[3 * Nd + i] / h;
+      const double u = U[Nd + i] / h, v = U[2 * Nd + i] / h, w = U[3 * Nd + i] / h;
       acc += wq * (0.5 * h * (u * u + v * v + (1.0 / a.gamma) * w * w + a.g * (h - 2.0 * Hnod[i])));
     }
   }
@@ -100,20 +100,12 @@ __global__ void __launch_bounds__(kThreads) k_diag_final(int what, const double*
   if (threadIdx.x == 0) out[0] = sh[0] * scale;
 }
 
-// Device address of the scratch array on the current device (set-up on first use).
+// Device address of the scratch array on the current device, looked up on every call.
 cudaError_t scratch_for_current_device(double** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
+  double* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_diag_scratch);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    double* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_diag_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_ptr[dev] = p;
-  }
-  *out = g_scratch_ptr[dev];
+  *out = p;
   return cudaSuccess;
 }
 

@@ -196,10 +196,11 @@ __global__ void __launch_bounds__(256) k_diag(int what, const RhsConsts C, const
   double acc = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < Nd;
        i += (long long)gridDim.x * blockDim.x) {
-    const double h = U[i], hu = U[Nd + i], hv = U[2 * Nd + i];
+    const double h = U[i];  // the mass reads h alone
     const int loc = (int)(i % 25);
     const double wq = q.w[loc % 5] * q.w[loc / 5];
     if (what == 0) {
+      const double hu = U[Nd + i], hv = U[2 * Nd + i];
       const double p = U[4 * Nd + i] / h;
       const double arg = C.g * h + p + C.c2;
       const double ce = sqrt(arg > 0.0 ? arg : 0.0);
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(256) k_diag(int what, const RhsConsts C, const
     } else if (what == 1) {
       acc += wq * h;
     } else {
-      const double u = hu / h, v = hv / h, w = U[3 * Nd + i] / h;
+      const double u = U[Nd + i] / h, v = U[2 * Nd + i] / h, w = U[3 * Nd + i] / h;
       const double e = 0.5 * h * (u * u + v * v + (1.0 / C.gamma) * w * w +
                                   C.g * (h - 2.0 * C.Hnod[i]));
       acc += wq * e;

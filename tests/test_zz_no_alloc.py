@@ -63,3 +63,29 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     assert _call(1, kw, x.data_ptr(), x.data_ptr(), x.data_ptr()) == 1
     kw = dict(kw, Nx=2048, Ny=1310)  # fits; not launched here (x is too small)
     assert 25 * 2048 * 1310 <= 67108864
+
+
+def test_noalloc_largest_accepted_mesh():
+    """The largest mesh the scratch array takes (2048 x 1310: 67,072,000 nodes per field,
+    16,375 of the 16,384 partial slots, the final pass folding 64 partials per thread):
+    the mass of a seeded depth field equals the quadrature-weighted sum formed by torch,
+    on two calls in a row."""
+    import torch
+
+    Nx, Ny, Lx, Ly = 2048, 1310, 40.0, 26.0
+    Nd = 25 * Nx * Ny
+    assert (Nd + 4095) // 4096 <= 16384
+    kw = dict(Nx=Nx, Ny=Ny, Lx=Lx, Ly=Ly, g=9.81, c=3.0 * np.sqrt(9.81), gamma=1.5)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    U = torch.zeros(5 * Nd, dtype=torch.float64, device="cuda")
+    U[:Nd] = 0.45 + 0.05 * torch.rand(Nd, generator=g, dtype=torch.float64, device="cuda")
+    qw = torch.tensor(sgnb.fr_tables()["qw"], dtype=torch.float64, device="cuda")
+    w = (qw[None, :] * qw[:, None]).reshape(25).repeat(Nx * Ny)  # node a + 5 b
+    ref = float((w * U[:Nd]).sum()) * (0.5 * Lx / Nx) * (0.5 * Ly / Ny)
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        out.fill_(np.nan)
+        torch.cuda.synchronize()
+        assert _call(1, kw, U.data_ptr(), U.data_ptr(), out.data_ptr()) == 0
+        torch.cuda.synchronize()
+        assert out.item() == pytest.approx(ref, rel=1e-12)
