@@ -469,6 +469,10 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
   const long long Nd = C.Nd;
   const int ex0 = bx * TX, ey0 = by * TY;
   const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
+  // the element columns and rows across the tile's edges, wrapped periodically (a compare
+  // instead of an integer remainder by the mesh size)
+  const int exL = ex0 == 0 ? Nx - 1 : ex0 - 1, exR = ex0 + TXv == Nx ? 0 : ex0 + TXv;
+  const int eyB = ey0 == 0 ? Ny - 1 : ey0 - 1, eyT = ey0 + TYv == Ny ? 0 : ey0 + TYv;
   // slab edges: the trace nodes across come from the neighbours' ghost arrays
   bool ghostL = false, ghostR = false;
   if constexpr (GHOST) {
@@ -547,20 +551,20 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       if (slot < TY) {
         if (GHOST && ghostL) hs[u] = 1;
         ok = ok && slot < TYv && !wallL;
-        e = (long long)((ex0 - 1 + Nx) % Nx) + (long long)Nx * (ey0 + slot);
+        e = (long long)(exL) + (long long)Nx * (ey0 + slot);
         node = (NP - 1) + NP * t;
       } else if (slot < 2 * TY) {
         if (GHOST && ghostR) hs[u] = 2;
         ok = ok && slot - TY < TYv && !wallR;
-        e = (long long)((ex0 + TXv) % Nx) + (long long)Nx * (ey0 + slot - TY);
+        e = (long long)(exR) + (long long)Nx * (ey0 + slot - TY);
         node = NP * t;
       } else if (slot < 2 * TY + TX) {
         ok = ok && slot - 2 * TY < TXv && !wallB;
-        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * ((ey0 - 1 + Ny) % Ny);
+        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * (eyB);
         node = t + NP * (NP - 1);
       } else {
         ok = ok && slot - 2 * TY - TX < TXv && !wallT;
-        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * ((ey0 + TYv) % Ny);
+        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * (eyT);
         node = t;
       }
       hq[u] = ok ? q : -1;
@@ -608,12 +612,12 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             const int ey = ey0 + slot;
 #ifdef SGNB_CHECKED
             const long long fe = (long long)ey * NP + t;
-            const long long fx = ((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t;
+            const long long fx = ((long long)(exR) + (long long)Nx * ey) * NP + t;
             fv[u] = (wallR || ghostR) ? (SGNB_INB(fe, (long long)Ny * NP) ? C.HfXEnd[fe] : 0.0)
                                       : (SGNB_INB(fx, Nd / NP) ? C.HfX[fx] : 0.0);
 #else
             fv[u] = (wallR || ghostR) ? C.HfXEnd[(long long)ey * NP + t]
-                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t];
+                          : C.HfX[((long long)(exR) + (long long)Nx * ey) * NP + t];
 #endif
             fq[u] = q;
           }
@@ -621,12 +625,12 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
           const int ex = ex0 + slot - TY;
 #ifdef SGNB_CHECKED
           const long long fe = (long long)ex * NP + t;
-          const long long fy = ((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t;
+          const long long fy = ((long long)ex + (long long)Nx * (eyT)) * NP + t;
           fv[u] = wallT ? (SGNB_INB(fe, (long long)Nx * NP) ? C.HfYEnd[fe] : 0.0)
                         : (SGNB_INB(fy, Nd / NP) ? C.HfY[fy] : 0.0);
 #else
           fv[u] = wallT ? C.HfYEnd[(long long)ex * NP + t]
-                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t];
+                        : C.HfY[((long long)ex + (long long)Nx * (eyT)) * NP + t];
 #endif
           fq[u] = q;
         }
