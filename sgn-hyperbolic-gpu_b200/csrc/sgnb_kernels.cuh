@@ -429,8 +429,10 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 // One tile of the fused right-hand side / stage kernel: tile (bx, by) of the mesh whose
 // constants are C, error partial slot blk. Shared by the single-instance kernel and the
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
+// FULL: the mesh is a whole number of tiles, so every tile is full and the per-item range
+// checks and their branches are compiled out (8 % off the end-point stage at 2048 x 1024).
 template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false,
-          bool GHOST = false, bool GAUSS = false>
+          bool GHOST = false, bool GAUSS = false, bool FULL = false>
 __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_, EXACT>::Smem& S) {
@@ -468,7 +470,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
   const int Nx = C.Nx, Ny = C.Ny;
   const long long Nd = C.Nd;
   const int ex0 = bx * TX, ey0 = by * TY;
-  const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
+  const int TXv = FULL ? TX : min(TX, Nx - ex0), TYv = FULL ? TY : min(TY, Ny - ey0);
   // the element columns and rows across the tile's edges, wrapped periodically (a compare
   // instead of an integer remainder by the mesh size)
   const int exL = ex0 == 0 ? Nx - 1 : ex0 - 1, exR = ex0 + TXv == Nx ? 0 : ex0 + TXv;
@@ -486,7 +488,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
   // item q = tid + NTHR*u is double k of tile row iy: global (e_row*25 + k), shared
   // iy*RUN + k (the [TE][NPP] layout of one field). Recomputed after the passes rather
   // than kept live through them.
-  long long gof[NIT];
+  int gof[NIT];  // node offset within one field (Nd <= 2^31 by the mesh-size limit)
   int sof[NIT];
   bool okk[NIT];
   auto item_map = [&]() {
@@ -494,8 +496,8 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NIT; ++u) {
       const int q = tid + NTHR * u;
       const int iy = q / RUN, k = q - iy * RUN;
-      okk[u] = iy < TYv && k < TXv * NPP;
-      gof[u] = ((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k;
+      okk[u] = FULL || (iy < TYv && k < TXv * NPP);
+      gof[u] = (int)(((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k);
       sof[u] = iy * RUN + k;
     }
   };
@@ -519,9 +521,9 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u] && SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) {
-            cp_async8(&(&S.U[v][0][0])[sof[u]], src + (long long)v * Nd + gof[u]);
+            cp_async8(&(&S.U[v][0][0])[sof[u]], (src + (long long)v * Nd) + gof[u]);
             if constexpr (MODE == MODE_STAGE)
-              cp_async8(&(&S.G[v][0][0])[sof[u]], I.k + (long long)v * Nd + gof[u]);
+              cp_async8(&(&S.G[v][0][0])[sof[u]], (I.k + (long long)v * Nd) + gof[u]);
           }
     } else {
       // end-point stage, round 1: k1 and k2 into the U and G areas
@@ -530,8 +532,8 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u] && SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) {
-            cp_async8(&(&S.U[v][0][0])[sof[u]], I.k1 + (long long)v * Nd + gof[u]);
-            cp_async8(&(&S.G[v][0][0])[sof[u]], I.k2 + (long long)v * Nd + gof[u]);
+            cp_async8(&(&S.U[v][0][0])[sof[u]], (I.k1 + (long long)v * Nd) + gof[u]);
+            cp_async8(&(&S.G[v][0][0])[sof[u]], (I.k2 + (long long)v * Nd) + gof[u]);
           }
     }
     // halo items: descriptors, then loads
@@ -664,7 +666,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u] && SGNB_INB(gof[u], Nd)) ux[v][u] = I.u[(long long)v * Nd + gof[u]];
+          if (okk[u] && SGNB_INB(gof[u], Nd)) ux[v][u] = (I.u + (long long)v * Nd)[gof[u]];
 #pragma unroll
       for (int v = 0; v < NV; ++v)
 #pragma unroll
@@ -673,7 +675,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             double& y = (&S.U[v][0][0])[sof[u]];
             y = fsal_part(y, (&S.G[v][0][0])[sof[u]]);
             if (SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP))
-              cp_async8(&(&S.G[v][0][0])[sof[u]], I.k3 + (long long)v * Nd + gof[u]);
+              cp_async8(&(&S.G[v][0][0])[sof[u]], (I.k3 + (long long)v * Nd) + gof[u]);
           }
       double* __restrict__ unew = A.U[cur ^ 1];  // stored evict-first (see the copy-out)
       cp_async_wait_all();
@@ -685,7 +687,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
             double& y = (&S.U[v][0][0])[sof[u]];
             const double un = fsal_finish(ux[v][u], y, (&S.G[v][0][0])[sof[u]], I.dt);
             y = un;
-            if (SGNB_INB(gof[u], Nd)) __stcs(&unew[(long long)v * Nd + gof[u]], un);
+            if (SGNB_INB(gof[u], Nd)) __stcs(&(unew + (long long)v * Nd)[gof[u]], un);
           }
       }
     }
@@ -694,7 +696,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 
   const int i = lane;  // tile element of this lane
   const int ix = i % TX, iy = i / TX;
-  const bool valid = ix < TXv && iy < TYv;
+  const bool valid = FULL || (ix < TXv && iy < TYv);
   const int j = warp;  // GLL line index of this warp
 
   // ---- column pass: y-line a = j ---------------------------------------------
@@ -863,7 +865,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
-          if (okk[u] && SGNB_INB(gof[u], Nd)) __stcs(&outp[(long long)v * Nd + gof[u]], (&S.G[v][0][0])[sof[u]]);
+          if (okk[u] && SGNB_INB(gof[u], Nd)) __stcs(&(outp + (long long)v * Nd)[gof[u]], (&S.G[v][0][0])[sof[u]]);
     } else {
       // One field at a time, with the next field's four arrays prefetched while the
       // current field's error is formed: hoisting every field's loads at once would
@@ -873,7 +875,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
-          const long long g = gof[u];
+          const int g = gof[u];
           if (SGNB_INB(g, Nd)) { uu[u] = __ldcs(&I.u[g]); c1[u] = __ldcs(&I.k1[g]); c2[u] = __ldcs(&I.k2[g]); c3[u] = __ldcs(&I.k3[g]); }
         }
 #pragma unroll 1
@@ -882,15 +884,16 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
           for (int u = 0; u < NIT; ++u)
             if (okk[u]) {
-              const long long g = (long long)(v + 1) * Nd + gof[u];
-              if (SGNB_INB(g, NV * Nd)) { nu[u] = __ldcs(&I.u[g]); n1[u] = __ldcs(&I.k1[g]); n2[u] = __ldcs(&I.k2[g]); n3[u] = __ldcs(&I.k3[g]); }
+              const long long o = (long long)(v + 1) * Nd;  // per-field base, 32-bit item offset
+              const int g = gof[u];
+              if (SGNB_INB(o + g, NV * Nd)) { nu[u] = __ldcs(&(I.u + o)[g]); n1[u] = __ldcs(&(I.k1 + o)[g]); n2[u] = __ldcs(&(I.k2 + o)[g]); n3[u] = __ldcs(&(I.k3 + o)[g]); }
             }
         }
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
             const double k4 = (&S.G[v][0][0])[sof[u]];
-            if (SGNB_INB(gof[u], Nd)) __stcs(&outp[(long long)v * Nd + gof[u]], k4);
+            if (SGNB_INB(gof[u], Nd)) __stcs(&(outp + (long long)v * Nd)[gof[u]], k4);
             // scaled embedded error, src/solver/rk.cpp:118-128; the candidate uNew is
             // still in the tile (the passes only read S.U)
             const double dt = I.dt;
@@ -987,12 +990,14 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 // frictionless kernels carry none of its code).
 // GHOST: slab edges compiled in (only contexts with ghost arrays launch these variants).
 // GAUSS: Gauss-Legendre points (after k_traces of the same stage).
-template <int MODE, bool EXACT, bool FRIC = false, bool GHOST = false, bool GAUSS = false>
+// FULL: Nx a multiple of 8 and Ny of 4 (every tile full).
+template <int MODE, bool EXACT, bool FRIC = false, bool GHOST = false, bool GAUSS = false,
+          bool FULL = false>
 __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(const RhsConsts C, const StageArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   using T = Tile<8, 4, EXACT>;
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
-  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC, GHOST, GAUSS>(C, C, A, blockIdx.x, blockIdx.y,
+  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC, GHOST, GAUSS, FULL>(C, C, A, blockIdx.x, blockIdx.y,
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 

@@ -25,22 +25,24 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
     else k_fused<MODE, SGNB_EXACT, true, false><<<grid, NTHR, smem, s>>>(C, A);
   } else {
     if (ghost) k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
+    else if (C.Nx % 8 == 0 && C.Ny % 4 == 0)  // every tile full
+      k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
     else k_fused<MODE, SGNB_EXACT, false, false><<<grid, NTHR, smem, s>>>(C, A);
   }
   return cudaGetLastError();
 }
 
-template <bool FRIC, bool GHOST, bool GAUSS = false>
+template <bool FRIC, bool GHOST, bool GAUSS = false, bool FULL = false>
 static cudaError_t prepare_variant() {
   const int bytes = (int)sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC, GHOST, GAUSS>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_RHS, SGNB_EXACT, FRIC, GHOST, GAUSS, FULL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC, GHOST, GAUSS>,
+  if ((e = cudaFuncSetAttribute(k_fused<MODE_STAGE, SGNB_EXACT, FRIC, GHOST, GAUSS, FULL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC, GHOST, GAUSS>,
+  return cudaFuncSetAttribute(k_fused<MODE_FSAL, SGNB_EXACT, FRIC, GHOST, GAUSS, FULL>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
@@ -51,6 +53,7 @@ static cudaError_t prepare_all() {
   if (e == cudaSuccess) e = prepare_variant<true, true>();
   if (e == cudaSuccess) e = prepare_variant<false, false, true>();
   if (e == cudaSuccess) e = prepare_variant<true, false, true>();
+  if (e == cudaSuccess) e = prepare_variant<false, false, false, true>();
   return e;
 }
 

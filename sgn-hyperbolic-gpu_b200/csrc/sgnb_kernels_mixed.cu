@@ -9,6 +9,8 @@ template <int MODE>
 static cudaError_t launch_m(const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
   const dim3 grid((C.Nx + mix::TX - 1) / mix::TX, (C.Ny + mix::TY - 1) / mix::TY);
   if (C.manning) mix::k_mixed<MODE, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  else if (C.Nx % mix::TX == 0 && C.Ny % mix::TY == 0)  // every tile full
+    mix::k_mixed<MODE, false, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
   else mix::k_mixed<MODE, false><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
   return cudaGetLastError();
 }
@@ -39,22 +41,23 @@ cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A
   }
 }
 
-template <bool FRIC>
+template <bool FRIC, bool FULL = false>
 static cudaError_t prepare_mixed_fric() {
   const int bytes = (int)sizeof(mix::Smem);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_RHS, FRIC>,
+  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_RHS, FRIC, FULL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_STAGE, FRIC>,
+  if ((e = cudaFuncSetAttribute(mix::k_mixed<mix::MODE_STAGE, FRIC, FULL>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(mix::k_mixed<mix::MODE_FSAL, FRIC>,
+  return cudaFuncSetAttribute(mix::k_mixed<mix::MODE_FSAL, FRIC, FULL>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 cudaError_t prepare_fused_mixed() {
   cudaError_t e = prepare_mixed_fric<false>();
+  if (e == cudaSuccess) e = prepare_mixed_fric<false, true>();
   return e == cudaSuccess ? prepare_mixed_fric<true>() : e;
 }
 

@@ -5,19 +5,30 @@
 //   FP64  the well-balanced hydrostatic flux 0.5 g (h^2 - H^2) of the normal momentum, its
 //         Rusanov central average, its FR-corrected derivative, and the bathymetry source
 //         g (h - H) grad H. These two cancel to O(g h grad eta); the cancellation happens
-//         in FP64 and only the result is rounded to FP32. The state, the RK stage
-//         combinations, the embedded error estimate and the controller are FP64 too.
-//   FP32  everything that is a deviation from the lake at rest: mass and advective
-//         fluxes, the hp and hw fluxes, Rusanov dissipation lam/2 (U_R - U_L) (the jump of h
-//         is formed in FP64 and rounded), wave speeds, the FR derivatives of these fluxes,
-//         the depth gradient D eta + grad H of the non-conservative products, and the
-//         sources gamma p grad H, gamma p, -2 c^2 (w + u H_x + v H_y).
+//         in FP64 and only the result is rounded to FP32. The terms linear in the
+//         discharges hu, hv: the mass flux hn and the c^2 hn part of the hp flux, their
+//         central face averages and FR-corrected derivatives, and the Rusanov jumps of h,
+//         hu and hv (formed in FP64, then rounded). hu and hv stay FP64 in shared memory:
+//         a 5-point derivative of FP32-rounded discharges puts grid-scale noise of
+//         relative size 2^-24 |D| / J into dh/dt, which the adaptive step sequence of
+//         configuration 1 amplifies past an eta error of 1e-6 (rounding only hw and hp, or
+//         only the stored k, stays near 1e-7). For the same reason the FR derivative of
+//         eta = h - H and the depth gradient D eta + grad H of the non-conservative
+//         products are FP64, and the 5-point derivatives of the momentum fluxes (which
+//         carry hp linearly) accumulate their FP32 flux values in FP64; each is rounded
+//         once, after the sum. The state, the RK stage combinations, the embedded error
+//         estimate and the controller are FP64 too.
+//   FP32  the remaining deviations from the lake at rest: the advective (quadratic)
+//         fluxes, the hw and hp fluxes apart from c^2 hn, the Rusanov dissipation
+//         lam/2 (U_R - U_L) of hw and hp, wave speeds, the FR derivatives of these fluxes,
+//         the products c^2 u h_x of the non-conservative terms, and the sources
+//         gamma p grad H, gamma p, -2 c^2 (w + u H_x + v H_y).
 // At rest every FP32 term is exactly zero, so the lake-at-rest residual is the FP64 one.
 // Stage derivatives k are stored in FP32 (the RK accumulation u + dt sum b_i k_i and the
 // error estimate promote them to FP64).
 //
 // Layout and work decomposition are those of sgnb_kernels.cuh (8 x 4 element tiles, 5 warps,
-// lane = element, warp = GLL line); shared memory is 63 KB, so 3 CTAs fit per SM.
+// lane = element, warp = GLL line); shared memory is 56.3 KB, so 3 CTAs fit per SM.
 #pragma once
 
 #include <cstdint>
@@ -45,10 +56,11 @@ enum : int { MODE_RHS = 0, MODE_STAGE = 1, MODE_FSAL = 2 };
 struct Smem {
   double h[TE][NPP];          // full depth (FP64)
   double H[TE][NPP];          // nodal still depth (its gradient is formed from it)
-  float q[4][TE][NPP];        // hu, hv, hw, hp (FP32 deviations)
+  double d[2][TE][NPP];       // hu, hv (FP64: their linear fluxes are formed in FP64)
+  float q[2][TE][NPP];        // hw, hp (FP32 deviations)
   float G[NV + 1][TE][NPP];   // column-pass results (dG incl. the y hydrostatic part, By)
-  double hhalo[NHALO * NP];   // halo depth, slot layout of sgnb_kernels.cuh
-  float qhalo[4 * NHALO * NP];
+  double hhalo[3 * NHALO * NP];  // halo h, hu, hv; slot layout of sgnb_kernels.cuh
+  float qhalo[2 * NHALO * NP];   // halo hw, hp
   double Hf[(2 * TE + TY + TX) * NP];
   double red[NWARP][3];
 };
@@ -129,15 +141,16 @@ __device__ __forceinline__ PtF make_pt(double h64, float hu, float hv, float hw,
   return s;
 }
 
-// FP32 (deviation) part of flux field v; the hydrostatic term is added in FP64 elsewhere.
+// FP32 (deviation) part of flux field v. The hydrostatic term of the normal momentum, the
+// mass flux hn and the c^2 hn part of the hp flux are formed in FP64 elsewhere.
 template <int DIR, class TC>
 __device__ __forceinline__ float flux_dev(const TC& C, int v, const PtF& s) {
   switch (v) {
-    case 0: return s.hn;
+    case 0: return 0.0f;
     case 1: return DIR == 0 ? s.hu * s.u + s.hp : s.hv * s.u;
     case 2: return DIR == 0 ? s.hu * s.v : s.hv * s.v + s.hp;
     case 3: return s.hn * s.w;
-    default: return s.hn * (s.p + (float)C.c2);
+    default: return s.hn * s.p;
   }
 }
 
@@ -154,36 +167,40 @@ __device__ __forceinline__ double hydro64(const TC& C, double h, double Hl) {
   return C.halfg * ((h - Hl) * (h + Hl));
 }
 
-// One GLL line: dyn[5] (FP32 FR derivatives of the deviation fluxes), hyd (FP64 FR
-// derivative of the hydrostatic flux of the normal momentum) and deta (FP32 FR derivative
-// of the depth with the central face depth). Emitted per node through the callbacks.
+// One GLL line: dyn[5] (FR derivatives of the fluxes: the FP64 linear parts plus the FP32
+// deviation parts, rounded once), hyd (FP64 FR derivative of the hydrostatic flux of the
+// normal momentum) and deta (FP64 FR derivative of eta = h - H with the central face depth:
+// a 5-point derivative of FP32-rounded eta would put grid-scale noise into the
+// non-conservative products, as a derivative of FP32 discharges would into dh/dt).
+// Emitted per node through the callbacks.
 //   h[k]      full depth at the nodes (FP64), Hn[k] nodal still depth
+//   hn[k]     FP64 normal discharge at the nodes; tLo64 / tHi64 the FP64 tangential
+//             discharge at the two face nodes
 //   qf[k][4]  FP32 hu, hv, hw, hp at the nodes
-//   nh, nq    the neighbour node across each face (FP64 depth, FP32 discharges)
+//   nd, nq    the neighbour node across each face: FP64 h, hu, hv and FP32 hw, hp
 template <int DIR, class TC, class TB, class EmitN, class Emit>
 __device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const double (&h)[NP],
-                                           const double (&Hn)[NP], const float (&qf)[NP][4],
-                                           double nhLo, const float* nqLo, double nhHi,
-                                           const float* nqHi, double HfLo, double HfHi,
-                                           EmitN&& emit_node, Emit&& emit) {
+                                           const double (&Hn)[NP], const double (&hn)[NP],
+                                           double tLo64, double tHi64, const float (&qf)[NP][4],
+                                           const double* ndLo, const float* nqLo,
+                                           const double* ndHi, const float* nqHi, double HfLo,
+                                           double HfHi, EmitN&& emit_node, Emit&& emit) {
   PtF s[NP];
-  float eta[NP];
   double hyd[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
     s[k] = make_pt<DIR>(h[k], qf[k][0], qf[k][1], qf[k][2], qf[k][3]);
-    eta[k] = (float)(h[k] - Hn[k]);
     hyd[k] = hydro64(C, h[k], Hn[k]);
   }
-  const PtF sLo = make_pt<DIR>(nhLo, nqLo[0], nqLo[1], nqLo[2], nqLo[3]);
-  const PtF sHi = make_pt<DIR>(nhHi, nqHi[0], nqHi[1], nqHi[2], nqHi[3]);
+  const PtF sLo = make_pt<DIR>(ndLo[0], (float)ndLo[1], (float)ndLo[2], nqLo[0], nqLo[1]);
+  const PtF sHi = make_pt<DIR>(ndHi[0], (float)ndHi[1], (float)ndHi[2], nqHi[0], nqHi[1]);
   const PtF& tLo = s[0];
   const PtF& tHi = s[NP - 1];
   // Rusanov, FP32 deviation part (sgn_flux2d.h:169-179)
   const float lamLo = fmaxf(wave_speed_f<DIR>(C, sLo), wave_speed_f<DIR>(C, tLo));
   const float lamHi = fmaxf(wave_speed_f<DIR>(C, tHi), wave_speed_f<DIR>(C, sHi));
-  // jumps of the conserved variables: h in FP64, rounded after the difference
-  const float dhLo = (float)(h[0] - nhLo), dhHi = (float)(nhHi - h[NP - 1]);
+  // jumps of the conserved variables: h, hu, hv in FP64, rounded after the difference
+  const float dhLo = (float)(h[0] - ndLo[0]), dhHi = (float)(ndHi[0] - h[NP - 1]);
   float jLo[NV], jHi[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
@@ -192,8 +209,14 @@ __device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const doub
     float duLo, duHi;  // own minus neighbour (low face), neighbour minus own (high face)
     switch (v) {
       case 0: duLo = dhLo; duHi = dhHi; break;
-      case 1: duLo = tLo.hu - sLo.hu; duHi = sHi.hu - tHi.hu; break;
-      case 2: duLo = tLo.hv - sLo.hv; duHi = sHi.hv - tHi.hv; break;
+      case 1:
+        duLo = (float)((DIR == 0 ? hn[0] : tLo64) - ndLo[1]);
+        duHi = (float)(ndHi[1] - (DIR == 0 ? hn[NP - 1] : tHi64));
+        break;
+      case 2:
+        duLo = (float)((DIR == 1 ? hn[0] : tLo64) - ndLo[2]);
+        duHi = (float)(ndHi[2] - (DIR == 1 ? hn[NP - 1] : tHi64));
+        break;
       case 3: duLo = tLo.hw - sLo.hw; duHi = sHi.hw - tHi.hw; break;
       default: duLo = tLo.hp - sLo.hp; duHi = sHi.hp - tHi.hp; break;
     }
@@ -201,23 +224,31 @@ __device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const doub
     jHi[v] = 0.5f * (FnHi - FdHi) - 0.5f * lamHi * duHi;
   }
   // hydrostatic jumps at the faces (FP64): central average minus own face value
-  const double jHydLo = 0.5 * (hydro64(C, nhLo, HfLo) - hydro64(C, h[0], HfLo));
-  const double jHydHi = 0.5 * (hydro64(C, nhHi, HfHi) - hydro64(C, h[NP - 1], HfHi));
+  const double jHydLo = 0.5 * (hydro64(C, ndLo[0], HfLo) - hydro64(C, h[0], HfLo));
+  const double jHydHi = 0.5 * (hydro64(C, ndHi[0], HfHi) - hydro64(C, h[NP - 1], HfHi));
+  // central jumps of the normal discharge (FP64): the mass flux hn and the c^2 hn part of
+  // the hp flux share its FR-corrected derivative dlin (their Rusanov dissipation, on h
+  // and on hp, is in the FP32 part)
+  const double jcLo = 0.5 * (ndLo[1 + DIR] - hn[0]);
+  const double jcHi = 0.5 * (ndHi[1 + DIR] - hn[NP - 1]);
   // depth jumps with the central common depth h* = (h- + h+)/2 (sgn2d.cpp:213-214)
-  const float jeLo = -0.5f * dhLo, jeHi = 0.5f * dhHi;
+  const double jeLo = -0.5 * (h[0] - ndLo[0]), jeHi = 0.5 * (ndHi[0] - h[NP - 1]);
   const float iJ = (float)(DIR == 0 ? C.iJx : C.iJy);
   const double iJ64 = DIR == 0 ? C.iJx : C.iJy;
+  double dlin[NP];
 #pragma unroll
   for (int m = 0; m < NP; ++m) {
-    const float gL = (float)Tb.gLp[m], gR = (float)Tb.gRp[m];
-    float se = jeLo * gL + jeHi * gR;
+    double se = jeLo * Tb.gLp[m] + jeHi * Tb.gRp[m];
     double sh = jHydLo * Tb.gLp[m] + jHydHi * Tb.gRp[m];
+    double sl = jcLo * Tb.gLp[m] + jcHi * Tb.gRp[m];
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      se = fmaf((float)Tb.D[m * NP + k], eta[k], se);
+      se = fma(Tb.D[m * NP + k], h[k] - Hn[k], se);
       sh = fma(Tb.D[m * NP + k], hyd[k], sh);
+      sl = fma(Tb.D[m * NP + k], hn[k], sl);
     }
-    emit_node(m, se * iJ, sh * iJ64, s[m], eta[m]);
+    dlin[m] = sl * iJ64;
+    emit_node(m, se * iJ64, sh * iJ64, s[m]);
   }
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
@@ -226,18 +257,35 @@ __device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const doub
     for (int k = 0; k < NP; ++k) F[k] = flux_dev<DIR>(C, v, s[k]);
 #pragma unroll
     for (int m = 0; m < NP; ++m) {
-      float a = jLo[v] * (float)Tb.gLp[m];
-      a = fmaf(jHi[v], (float)Tb.gRp[m], a);
+      float d;
+      if (v == 1 || v == 2) {
+        // the momentum fluxes carry hp linearly (|hp| grows to ~10 |hu| on configuration
+        // 1): their FP32 values are contracted in FP64, rounded once
+        double a = (double)jLo[v] * Tb.gLp[m];
+        a = fma((double)jHi[v], Tb.gRp[m], a);
 #pragma unroll
-      for (int k = 0; k < NP; ++k) a = fmaf((float)Tb.D[m * NP + k], F[k], a);
-      emit(m, v, a * iJ, s[m]);
+        for (int k = 0; k < NP; ++k) a = fma(Tb.D[m * NP + k], (double)F[k], a);
+        d = (float)(a * iJ64);
+      } else {
+        float a = jLo[v] * (float)Tb.gLp[m];
+        a = fmaf(jHi[v], (float)Tb.gRp[m], a);
+        if (v != 0) {
+#pragma unroll
+          for (int k = 0; k < NP; ++k) a = fmaf((float)Tb.D[m * NP + k], F[k], a);
+        }
+        d = a * iJ;
+      }
+      if (v == 0) d = (float)(dlin[m] + (double)d);
+      else if (v == NV - 1) d = (float)(C.c2 * dlin[m] + (double)d);
+      emit(m, v, d, s[m]);
     }
   }
 }
 
 // One tile (bx, by) of the mixed-precision right-hand side / stage kernel, error partial
-// slot blk. Shared by the single-instance kernel and the batched kernel.
-template <int MODE, class TC, class TB, class TA, bool FRIC = false>
+// slot blk. Shared by the single-instance kernel and the batched kernel. FULL: the mesh is
+// a whole number of tiles (the per-item range checks are compiled out).
+template <int MODE, class TC, class TB, class TA, bool FRIC = false, bool FULL = false>
 __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& A, int bx, int by,
                                            long long blk, Smem& S) {
 
@@ -267,7 +315,11 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   const int Nx = C.Nx, Ny = C.Ny;
   const long long Nd = C.Nd;
   const int ex0 = bx * TX, ey0 = by * TY;
-  const int TXv = min(TX, Nx - ex0), TYv = min(TY, Ny - ey0);
+  const int TXv = FULL ? TX : min(TX, Nx - ex0), TYv = FULL ? TY : min(TY, Ny - ey0);
+  // the element columns and rows across the tile's edges, wrapped periodically (a compare
+  // instead of an integer remainder by the mesh size)
+  const int exL = ex0 == 0 ? Nx - 1 : ex0 - 1, exR = ex0 + TXv == Nx ? 0 : ex0 + TXv;
+  const int eyB = ey0 == 0 ? Ny - 1 : ey0 - 1, eyT = ey0 + TYv == Ny ? 0 : ey0 + TYv;
   const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
   const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
 
@@ -279,7 +331,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NIT; ++u) {
       const int q = tid + NTHR * u;
       const int iy = q / RUN, k = q - iy * RUN;
-      okk[u] = iy < TYv && k < TXv * NPP;
+      okk[u] = FULL || (iy < TYv && k < TXv * NPP);
       gof[u] = ((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k;
       sof[u] = iy * RUN + k;
     }
@@ -307,11 +359,15 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
                          "l"(I.k + (long long)v * Nd + gof[u]) : "memory");
           }
     }
-    // end-point stage: k1 and k2 by asynchronous copies into the (still unused) G and q
-    // areas, ten FP32 fields
+    // end-point stage: k1 and k2 by asynchronous copies into the (still unused) G, q and d
+    // areas, ten FP32 fields: those of fields 0, 1, 2 in G (never written while the
+    // candidate is formed), of field 3 in q (hw and hp, written by the same thread at the
+    // same index after their read), of field 4 in d viewed as floats (written, as doubles
+    // at other indices, only after a barrier that follows every read)
     auto k12_slot = [&](int w, int v) -> float* {  // w: 0 = k1, 1 = k2
-      const int f = 5 * w + v;                     // G[0..5] then q[0..3]
-      return f < NV + 1 ? &S.G[f][0][0] : &S.q[f - NV - 1][0][0];
+      if (v < 3) return &S.G[2 * v + w][0][0];
+      if (v == 3) return &S.q[w][0][0];
+      return reinterpret_cast<float*>(&S.d[0][0][0]) + w * TE * NPP;
     };
     if constexpr (MODE == MODE_FSAL) {
 #pragma unroll
@@ -341,8 +397,12 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           }
       cp_async_wait_all();  // k (k1, k2) and the statics have landed
     }
+    // fields in the order 3, 4, 0, 1, 2: the end-point stage's field-4 derivatives sit in
+    // the d area, which fields 1 and 2 overwrite after the barrier
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
+    for (int o = 0; o < NV; ++o) {
+      const int v = (o + 3) % NV;
+      if (MODE == MODE_FSAL && v == 1) __syncthreads();
       double x[NIT];
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
@@ -359,7 +419,8 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           if (v == 0) (&S.h[0][0])[sof[u]] = x[u];
-          else (&S.q[v - 1][0][0])[sof[u]] = (float)x[u];
+          else if (v < 3) (&S.d[v - 1][0][0])[sof[u]] = x[u];
+          else (&S.q[v - 3][0][0])[sof[u]] = (float)x[u];
           if constexpr (MODE == MODE_FSAL)
             if (SGNB_INB(gof[u], Nd)) __stcs(&unew[(long long)v * Nd + gof[u]], x[u]);
         }
@@ -378,19 +439,19 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       int node = 0;
       if (slot < TY) {
         ok = ok && slot < TYv && !wallL;
-        e = (long long)((ex0 - 1 + Nx) % Nx) + (long long)Nx * (ey0 + slot);
+        e = (long long)(exL) + (long long)Nx * (ey0 + slot);
         node = (NP - 1) + NP * t;
       } else if (slot < 2 * TY) {
         ok = ok && slot - TY < TYv && !wallR;
-        e = (long long)((ex0 + TXv) % Nx) + (long long)Nx * (ey0 + slot - TY);
+        e = (long long)(exR) + (long long)Nx * (ey0 + slot - TY);
         node = NP * t;
       } else if (slot < 2 * TY + TX) {
         ok = ok && slot - 2 * TY < TXv && !wallB;
-        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * ((ey0 - 1 + Ny) % Ny);
+        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * (eyB);
         node = t + NP * (NP - 1);
       } else {
         ok = ok && slot - 2 * TY - TX < TXv && !wallT;
-        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * ((ey0 + TYv) % Ny);
+        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * (eyT);
         node = t;
       }
       hq[u] = ok ? q : -1;
@@ -420,20 +481,20 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           if (slot < TYv) {
             const int ey = ey0 + slot;
             fv[u] = SGNB_INB(wallR ? (long long)ey * NP + t
-                                   : ((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t,
+                                   : ((long long)(exR) + (long long)Nx * ey) * NP + t,
                              wallR ? (long long)Ny * NP : Nd / NP)
                         ? (wallR ? C.HfXEnd[(long long)ey * NP + t]
-                          : C.HfX[((long long)((ex0 + TXv) % Nx) + (long long)Nx * ey) * NP + t])
+                          : C.HfX[((long long)(exR) + (long long)Nx * ey) * NP + t])
                         : 0.0;
             fq[u] = q;
           }
         } else if (slot - TY < TXv) {
           const int ex = ex0 + slot - TY;
           fv[u] = SGNB_INB(wallT ? (long long)ex * NP + t
-                                 : ((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t,
+                                 : ((long long)ex + (long long)Nx * (eyT)) * NP + t,
                            wallT ? (long long)Nx * NP : Nd / NP)
                       ? (wallT ? C.HfYEnd[(long long)ex * NP + t]
-                        : C.HfY[((long long)ex + (long long)Nx * ((ey0 + TYv) % Ny)) * NP + t])
+                        : C.HfY[((long long)ex + (long long)Nx * (eyT)) * NP + t])
                       : 0.0;
           fq[u] = q;
         }
@@ -444,8 +505,8 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       if (hq[u] >= 0 && SGNB_INB(hq[u], NV * NHALO * NP)) {
         const int q = hq[u];
         const int v = q / (NHALO * NP), rest = q - v * NHALO * NP;
-        if (v == 0) S.hhalo[rest] = hv[u];
-        else S.qhalo[(v - 1) * NHALO * NP + rest] = (float)hv[u];
+        if (v < 3) S.hhalo[v * NHALO * NP + rest] = hv[u];
+        else S.qhalo[(v - 3) * NHALO * NP + rest] = (float)hv[u];
       }
 #pragma unroll
     for (int u = 0; u < NFIT; ++u)
@@ -456,57 +517,69 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
 
   const int i = lane;
   const int ix = i % TX, iy = i / TX;
-  const bool valid = ix < TXv && iy < TYv;
+  const bool valid = FULL || (ix < TXv && iy < TYv);
   const int j = warp;
   const float c2f = (float)C.c2, mc2f = (float)C.mc2, gammaf = (float)C.gamma;
 
-  // neighbour node across a face: in the tile, in the halo, or the wall mirror
-  auto halo_node = [&](int slot, int t, double& hh, float* qq) {
+  // neighbour node across a face: in the tile, in the halo, or the wall mirror (normal
+  // discharge negated, nd[1 + DIR])
+  auto halo_node = [&](int slot, int t, double* nd, float* nq) {
     const int idx = t + NP * slot;
-    hh = S.hhalo[idx];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) qq[c] = S.qhalo[c * NHALO * NP + idx];
+    for (int c = 0; c < 3; ++c) nd[c] = S.hhalo[c * NHALO * NP + idx];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) nq[c] = S.qhalo[c * NHALO * NP + idx];
   };
-  auto tile_node = [&](int e, int loc, double& hh, float* qq) {
-    hh = S.h[e][loc];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) qq[c] = S.q[c][e][loc];
+  auto tile_node = [&](int e, int loc, double* nd, float* nq) {
+    nd[0] = S.h[e][loc];
+    nd[1] = S.d[0][e][loc];
+    nd[2] = S.d[1][e][loc];
+    nq[0] = S.q[0][e][loc];
+    nq[1] = S.q[1][e][loc];
+  };
+  auto mirror_node = [&](int dir, double hh, double hu, double hv, const float* qq, double* nd,
+                         float* nq) {
+    nd[0] = hh;
+    nd[1] = dir == 0 ? -hu : hu;
+    nd[2] = dir == 1 ? -hv : hv;
+    nq[0] = qq[2];
+    nq[1] = qq[3];
   };
 
   // ---- column pass: y-line a = j ---------------------------------------------
   if (valid) {
-    double h[NP], Hn[NP];
+    double h[NP], Hn[NP], hn[NP];
     float qf[NP][4];
 #pragma unroll
     for (int b = 0; b < NP; ++b) {
       const int loc = j + NP * b;
       h[b] = S.h[i][loc];
       Hn[b] = S.H[i][loc];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) qf[b][c] = S.q[c][i][loc];
+      hn[b] = S.d[1][i][loc];
+      qf[b][0] = (float)S.d[0][i][loc];
+      qf[b][1] = (float)hn[b];
+      qf[b][2] = S.q[0][i][loc];
+      qf[b][3] = S.q[1][i][loc];
     }
-    double nhLo, nhHi;
-    float nqLo[4], nqHi[4];
-    if (iy > 0) tile_node(i - TX, j + NP * (NP - 1), nhLo, nqLo);
-    else if (wallB) {
-      nhLo = h[0];
-      nqLo[0] = qf[0][0]; nqLo[1] = -qf[0][1]; nqLo[2] = qf[0][2]; nqLo[3] = qf[0][3];
-    } else halo_node(2 * TY + ix, j, nhLo, nqLo);
-    if (iy + 1 < TYv) tile_node(i + TX, j, nhHi, nqHi);
-    else if (wallT) {
-      nhHi = h[NP - 1];
-      nqHi[0] = qf[NP - 1][0]; nqHi[1] = -qf[NP - 1][1]; nqHi[2] = qf[NP - 1][2]; nqHi[3] = qf[NP - 1][3];
-    } else halo_node(2 * TY + TX + ix, j, nhHi, nqHi);
+    const double tLo64 = S.d[0][i][j], tHi64 = S.d[0][i][j + NP * (NP - 1)];
+    double ndLo[3], ndHi[3];
+    float nqLo[2], nqHi[2];
+    if (iy > 0) tile_node(i - TX, j + NP * (NP - 1), ndLo, nqLo);
+    else if (wallB) mirror_node(1, h[0], tLo64, hn[0], qf[0], ndLo, nqLo);
+    else halo_node(2 * TY + ix, j, ndLo, nqLo);
+    if (iy + 1 < TYv) tile_node(i + TX, j, ndHi, nqHi);
+    else if (wallT) mirror_node(1, h[NP - 1], tHi64, hn[NP - 1], qf[NP - 1], ndHi, nqHi);
+    else halo_node(2 * TY + TX + ix, j, ndHi, nqHi);
     const double HfLo = hf_y(S, i, j);
     const double HfHi = (iy + 1 < TYv) ? hf_y(S, i + TX, j) : hf_yt(S, ix, j);
     float hydv[NP];
     line_mixed<1>(
-        C, Tb, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
-        [&](int b, float deta, double dhyd, const PtF& s, float) {
+        C, Tb, h, Hn, hn, tLo64, tHi64, qf, ndLo, nqLo, ndHi, nqHi, HfLo, HfHi,
+        [&](int b, double deta, double dhyd, const PtF& s) {
           const int loc = j + NP * b;
           const double Hyl = depth_grad<1>(C, Tb, S.H[i], j, b);
-          // ncpY with h_y = D eta + H_y (sgn_flux2d.h:156-161)
-          S.G[NV][i][loc] = mc2f * s.v * (deta + (float)Hyl);
+          // ncpY with h_y = D eta + H_y (sgn_flux2d.h:156-161), the sum in FP64
+          S.G[NV][i][loc] = mc2f * s.v * (float)(deta + Hyl);
           // y hydrostatic part of dU[HV]: -d_y hyd + g (h - H) H_y, cancelled in FP64
           hydv[b] = (float)(C.g * (h[b] - Hn[b]) * Hyl - dhyd);
         },
@@ -518,36 +591,36 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
 
   // ---- row pass: x-line b = j, then assembly ---------------------------------
   if (valid) {
-    double h[NP], Hn[NP];
+    double h[NP], Hn[NP], hn[NP];
     float qf[NP][4];
 #pragma unroll
     for (int a = 0; a < NP; ++a) {
       const int loc = a + NP * j;
       h[a] = S.h[i][loc];
       Hn[a] = S.H[i][loc];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) qf[a][c] = S.q[c][i][loc];
+      hn[a] = S.d[0][i][loc];
+      qf[a][0] = (float)hn[a];
+      qf[a][1] = (float)S.d[1][i][loc];
+      qf[a][2] = S.q[0][i][loc];
+      qf[a][3] = S.q[1][i][loc];
     }
-    double nhLo, nhHi;
-    float nqLo[4], nqHi[4];
-    if (ix > 0) tile_node(i - 1, (NP - 1) + NP * j, nhLo, nqLo);
-    else if (wallL) {
-      nhLo = h[0];
-      nqLo[0] = -qf[0][0]; nqLo[1] = qf[0][1]; nqLo[2] = qf[0][2]; nqLo[3] = qf[0][3];
-    } else halo_node(iy, j, nhLo, nqLo);
-    if (ix + 1 < TXv) tile_node(i + 1, NP * j, nhHi, nqHi);
-    else if (wallR) {
-      nhHi = h[NP - 1];
-      nqHi[0] = -qf[NP - 1][0]; nqHi[1] = qf[NP - 1][1]; nqHi[2] = qf[NP - 1][2]; nqHi[3] = qf[NP - 1][3];
-    } else halo_node(TY + iy, j, nhHi, nqHi);
+    const double tLo64 = S.d[1][i][NP * j], tHi64 = S.d[1][i][(NP - 1) + NP * j];
+    double ndLo[3], ndHi[3];
+    float nqLo[2], nqHi[2];
+    if (ix > 0) tile_node(i - 1, (NP - 1) + NP * j, ndLo, nqLo);
+    else if (wallL) mirror_node(0, h[0], hn[0], tLo64, qf[0], ndLo, nqLo);
+    else halo_node(iy, j, ndLo, nqLo);
+    if (ix + 1 < TXv) tile_node(i + 1, NP * j, ndHi, nqHi);
+    else if (wallR) mirror_node(0, h[NP - 1], hn[NP - 1], tHi64, qf[NP - 1], ndHi, nqHi);
+    else halo_node(TY + iy, j, ndHi, nqHi);
     const double HfLo = hf_x(S, i, j);
     const double HfHi = (ix + 1 < TXv) ? hf_x(S, i + 1, j) : hf_xr(S, iy, j);
     float hydu[NP], Bx[NP], Hxf[NP];
     line_mixed<0>(
-        C, Tb, h, Hn, qf, nhLo, nqLo, nhHi, nqHi, HfLo, HfHi,
-        [&](int a, float deta, double dhyd, const PtF& s, float) {
+        C, Tb, h, Hn, hn, tLo64, tHi64, qf, ndLo, nqLo, ndHi, nqHi, HfLo, HfHi,
+        [&](int a, double deta, double dhyd, const PtF& s) {
           const double Hxl = depth_grad<0>(C, Tb, S.H[i], a, j);
-          Bx[a] = mc2f * s.u * (deta + (float)Hxl);  // ncpX
+          Bx[a] = mc2f * s.u * (float)(deta + Hxl);  // ncpX, h_x summed in FP64
           hydu[a] = (float)(C.g * (h[a] - Hn[a]) * Hxl - dhyd);
           Hxf[a] = (float)Hxl;
         },
@@ -680,11 +753,17 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   }
 }
 
-template <int MODE, bool FRIC = false>
-__global__ void __launch_bounds__(NTHR, 3) k_mixed(const RhsConsts C, const StageArgsM A) {
+// Resident CTAs per SM the single-instance mixed kernels are compiled for (3 -> at most
+// 128 registers per thread, 2 -> 204).
+#ifndef SGNB_MIXED_MIN_CTAS
+#define SGNB_MIXED_MIN_CTAS 3
+#endif
+
+template <int MODE, bool FRIC = false, bool FULL = false>
+__global__ void __launch_bounds__(NTHR, SGNB_MIXED_MIN_CTAS) k_mixed(const RhsConsts C, const StageArgsM A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
-  mixed_tile<MODE, RhsConsts, RhsConsts, StageArgsM, FRIC>(
+  mixed_tile<MODE, RhsConsts, RhsConsts, StageArgsM, FRIC, FULL>(
       C, C, A, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
