@@ -14,8 +14,19 @@ README.md:369-377 and apps/sgn_bench.cu:138-141 of the reference).
 Our arm prints one JSON line with value (device-resident, CUDA events over K steps,
 max over ranks), e2e (the public API with host buffers: upload from pinned memory,
 K steps, download), roofline of the dominant kernel, clocks, the CPU baseline (the
-oracle port on rank 0) and the number of kernel launches. N > 1 runs independent
-replicas, one per GPU (the path does not exchange data between instances).
+oracle port on rank 0: three right-hand sides of the full state, and under "loop" the
+reference's integrateAdaptive on a row strip) and the number of kernel launches. N > 1
+runs independent replicas, one per GPU (the path does not exchange data between
+instances). At N = 1 the line also carries, each measured after the main run on its own
+contexts (--no-extras skips them):
+  mixed          configuration 2 in the mixed-precision mode against FP64 in the same run,
+                 the eta errors of both step sequences, and the exact mode's final-state
+                 sha256 with the fast mode's relative difference;
+  batched        configuration 4's 256-instance sweep, batched against the same instances
+                 run one after another;
+  adjoint        configuration 5's forward and VJP times and a central-difference check;
+  reference_gpu  the reference's own single-GPU solver (SGN2DCuda::integrateAdaptive,
+                 oracle/_ref/ref_gpu_bench) on configuration 2 with periodic boundaries.
 
 The reference arm times the reference's own CPU solver (oracle/_ref, compiled from the
 reference sources; the oracle port when that build is absent) on all host cores as
@@ -263,6 +274,20 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(U_np, kw, dof)
+        cpu["loop"] = cpu_baseline_loop(args)
+    solver.close()
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        # measured after the main run, each on its own contexts (the main solver is closed)
+        from sgnb import benchmarks as BW
+
+        extras = BW.default_extras(args, ClockSampler, (peak, peak_kind))
+        t0 = time.perf_counter()
+        try:
+            extras["reference_gpu"] = run_reference_gpu(args, summary=True)
+        except Exception as e:
+            extras["reference_gpu"] = {"error": f"{type(e).__name__}: {e}"}
+        extras["reference_gpu"]["wall_s"] = round(time.perf_counter() - t0, 1)
 
     if rank == 0:
         line = {
@@ -289,8 +314,8 @@ def run_ours(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
-    solver.close()
     if dist is not None:
         dist.destroy_process_group()
 
@@ -311,6 +336,34 @@ def cpu_baseline_port(U, kw, dof):
     return {"value": dof * n / t, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{n} rhs evaluation(s) of the full configuration-2 state "
                       f"(262,144,000 DOF) after one untimed one, {t:.1f} s"}
+
+
+def cpu_baseline_loop(args, rows=32, span=0.3):
+    """The reference's adaptive loop (integrateAdaptive, src/solver/rk.cpp:67-164, through
+    oracle/_ref when it was built, else the oracle port) on 1 host core over
+    [0, span x dt_CFL0.5] of a 2048 x `rows` periodic row strip of the configuration-2 mesh
+    (same element size; every right-hand side, stage combination and error norm of the loop
+    timed). The waves are not periodic across the strip's seam, so the controller settles
+    near dt_CFL0.5 / 16: a span of 0.3 is a handful of accepted steps (about 6 s)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from sgnb import workloads as W
+
+    use_ref = O.reference_available()
+    kw = W.cfg2_solver_args(2048, rows, 40.0, 20.0 * rows / 1024)
+    kw.update(bc_x=0, bc_y=0)
+    o = O.Oracle(reference=use_ref, **kw)
+    U = W.cfg2_state_torch(2048, rows, 40.0, 20.0 * rows / 1024, device="cpu").numpy()
+    dt0 = o.cfl_time_step(U, 0.5)
+    t0 = time.perf_counter()
+    _, st, _ = o.integrate_adaptive(U, 0.0, span * dt0, dt0)
+    t = time.perf_counter() - t0
+    dof = 5 * o.Nd
+    return {"value": dof * st["rhsEvals"] / t, "unit": UNIT, "cores": 1,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"integrateAdaptive over [0, {span} x dt_CFL0.5] of a 2048x{rows} "
+                      f"periodic strip ({dof:,} DOF): {st['accepted']} accepted, "
+                      f"{st['rejected']} rejected, {st['rhsEvals']} rhs, {t:.1f} s"}
 
 
 # --------------------------------------------------------------------------- reference arm
@@ -346,15 +399,19 @@ def _ref_worker(args):
     return time.perf_counter() - t0, 5 * o.Nd
 
 
-def run_reference_gpu(args):
+def run_reference_gpu(args, summary=False):
     """The reference's single-GPU solver (SGN2DCuda::integrateAdaptive, compiled from its
-    sources by oracle/Makefile) on configuration 2 with periodic boundaries."""
+    sources by oracle/Makefile) on configuration 2 with periodic boundaries. summary: return
+    the measurement (for the default line) instead of printing the reference line."""
     from sgnb import workloads as W
 
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_bench")
     if not os.path.exists(exe):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_gpu_bench not "
-                          "built (make -C oracle refgpu needs the reference sources)"}))
+        why = ("oracle/_ref/ref_gpu_bench not built (make -C oracle refgpu needs the "
+               "reference sources)")
+        if summary:
+            return {"unavailable": why}
+        print(json.dumps({"impl": "reference", "unavailable": why}))
         return
     Nx, Ny, Lx, Ly = W.CFG2["Nx"], W.CFG2["Ny"], W.CFG2["Lx"], W.CFG2["Ly"]
     if args.mesh:
@@ -367,6 +424,12 @@ def run_reference_gpu(args):
     with ClockSampler(0) as clk:
         out = subprocess.run(argv, check=True, capture_output=True, text=True).stdout
     r = json.loads(out.strip().splitlines()[-1])
+    if summary:
+        return {"solver": r["solver"], "value": r["value"], "unit": UNIT,
+                "ms_per_step": r["time_s"] / max(r["accepted"], 1) * 1e3,
+                "accepted": r["accepted"], "rejected": r["rejected"],
+                "rhs_evals": r["rhsEvals"], "boundaries": "periodic (the reference's only kind)",
+                "mesh": r["mesh"], "clocks": clk.summary()}
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
         "n_gpus": 1, "steps": int(r["accepted"]), "warmup": 1,
@@ -440,6 +503,9 @@ def main():
                          "configuration 5 forward + VJP; slabs: configuration 2 on x slabs "
                          "of one device against the whole mesh")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the sub-records of the default line (mixed, batched, adjoint, "
+                         "reference GPU solver), e.g. for profiler captures")
     ap.add_argument("--bc", choices=["walls", "periodic"], default="walls",
                     help="boundaries of configuration 2 (periodic: the reference solver's "
                          "only kind, for the comparison with --ref-device gpu)")
@@ -454,18 +520,11 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "sweep":
+    elif args.workload in ("sweep", "mixed", "adjoint", "slabs"):
         from sgnb import benchmarks as BW
-        BW.run_sweep(args, ClockSampler, measured_peak_hbm())
-    elif args.workload == "mixed":
-        from sgnb import benchmarks as BW
-        BW.run_mixed(args, ClockSampler, measured_peak_hbm())
-    elif args.workload == "adjoint":
-        from sgnb import benchmarks as BW
-        BW.run_adjoint(args, ClockSampler, measured_peak_hbm())
-    elif args.workload == "slabs":
-        from sgnb import benchmarks as BW
-        BW.run_slabs(args, ClockSampler, measured_peak_hbm())
+        fn = {"sweep": BW.run_sweep, "mixed": BW.run_mixed, "adjoint": BW.run_adjoint,
+              "slabs": BW.run_slabs}[args.workload]
+        print(json.dumps(fn(args, ClockSampler, measured_peak_hbm())), flush=True)
     else:
         run_ours(args)
 

@@ -1,7 +1,8 @@
 """Measurements of the batched sweep, the mixed-precision form and the adjoint, each
-printing one JSON line in the format of bench.py (which dispatches here with
---workload sweep | mixed | adjoint). Every number is taken on the device with CUDA events
-on the stream the work runs on, after warm-up, with the state resident in HBM.
+returning one JSON line in the format of bench.py (which prints it for --workload
+sweep | mixed | adjoint | slabs, and folds a summary of the first three into its default
+line through default_extras). Every number is taken on the device with CUDA events on the
+stream the work runs on, after warm-up, with the state resident in HBM.
 
 sweep    configuration 4: 256 instances (workloads.cfg4_instances) advanced K accepted
          steps each by the batched launches (after the autotuner), against the same
@@ -18,7 +19,7 @@ adjoint  configuration 5: the frozen 200-step trajectory with 16 gauges (forward
 """
 from __future__ import annotations
 
-import json
+import hashlib
 import math
 import time
 
@@ -33,6 +34,16 @@ UNIT = "DOF-updates/s"
 # end-point stage; nodal depth gradients formed on chip): FP64 and mixed precision
 STAGE_LOOP_BYTES = 2 * 26.24 + 50.24
 MIXED_LOOP_BYTES = 2 * 18.24 + 34.24
+
+
+def _rel_per_field(a, b):
+    """max over fields of max|a - b| / max|b| (each field's error over its largest value)."""
+    a, b = a.view(5, -1), b.view(5, -1)
+    out = 0.0
+    for v in range(5):
+        s = float(b[v].abs().max())
+        out = max(out, float((a[v] - b[v]).abs().max()) / (s if s > 0 else 1.0))
+    return out
 
 
 def _events(torch, stream=None):
@@ -119,7 +130,7 @@ def run_sweep(args, clock_sampler, peak):
         "gpu_launches": int(st[0].kernel_launches),
     }
     b.close()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_mixed(args, clock_sampler, peak):
@@ -136,6 +147,7 @@ def run_mixed(args, clock_sampler, peak):
     res = {}
     seqs = {}
     finals = {"adaptive": {}, "stable": {}}
+    full = {}
     clocks = None
     for name, prec in (("fp64", FP64_FAST), ("mixed", MIXED), ("exact", FP64_EXACT)):
         with SGN2DB200(precision=prec, **kw) as d:
@@ -168,6 +180,8 @@ def run_mixed(args, clock_sampler, peak):
                 try:
                     d.bs3_steps(0.0, dts)
                     finals[key][name] = d.state_tensor()[: d.Nd].clone()  # h
+                    if key == "adaptive" and name in ("fp64", "exact"):
+                        full[name] = d.state_tensor().clone()
                 except SgnbError:  # the replay left the stable range (non-finite state)
                     finals[key][name] = None
 
@@ -188,6 +202,15 @@ def run_mixed(args, clock_sampler, peak):
                                     "limit: round-off of any kind is amplified)"},
         "how": "each mode replays the step sequence from the same state (bs3 steps)",
     }
+    # fingerprint of the exact mode's final state (bit-identical to the reference's CPU
+    # solver on the same steps) and the fast mode's largest relative difference per field
+    if "exact" in full:
+        ex = full["exact"].cpu().numpy()
+        errors["exact_state"] = {
+            "sha256": hashlib.sha256(ex.tobytes()).hexdigest(),
+            "steps": int(len(seqs["adaptive"])),
+            "fast_rel_diff_per_field": (
+                _rel_per_field(full["fp64"], full["exact"]) if "fp64" in full else None)}
     ratio = res["mixed"]["value"] / res["fp64"]["value"]
     achieved = MIXED_LOOP_BYTES * res["mixed"]["value"] / 3.0 / 1e9  # bytes per attempt
     line = {
@@ -206,7 +229,7 @@ def run_mixed(args, clock_sampler, peak):
         "clocks": clocks,
         "gpu_launches": int(res["mixed"]["launches"]),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_adjoint(args, clock_sampler, peak):
@@ -277,7 +300,7 @@ def run_adjoint(args, clock_sampler, peak):
     }
     A.close()
     d.close()
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_slabs(args, clock_sampler, peak):
@@ -380,4 +403,48 @@ def run_slabs(args, clock_sampler, peak):
         "timing": "CUDA events on the solver's stream around the K steps (the host launches "
                   "every stage and reads the controller every 4 attempts)",
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def default_extras(args, clock_sampler, peak):
+    """Summaries of the mixed-precision, batched and adjoint measurements for the default
+    benchmark line, each with the same K and W as the main measurement (the adjoint's
+    timing repeats at most 3 times). A measurement that fails records its error instead."""
+    import copy
+    import gc
+
+    import torch
+
+    out = {}
+    a = copy.copy(args)
+    a.mesh, a.precision = None, "fast"
+
+    def timed(name, fn, summary):
+        t0 = time.perf_counter()
+        try:
+            r = summary(fn(a, clock_sampler, peak))
+        except Exception as e:  # recorded, the main measurement stands
+            r = {"error": f"{type(e).__name__}: {e}"}
+        r["wall_s"] = round(time.perf_counter() - t0, 1)
+        out[name] = r
+        gc.collect()
+        torch.cuda.empty_cache()
+
+    timed("mixed", run_mixed, lambda m: {
+        "value": m["value"], "fp64_value_same_run": m["fp64"]["value"],
+        "ratio_vs_fp64": m["speedup_vs_fp64"], "steps": m["steps"],
+        "eta_error": m["eta_error"], "roofline": m["roofline"], "clocks": m["clocks"]})
+    timed("batched", run_sweep, lambda s: {
+        "value": s["value"], "sequential_value": s["sequential_single_instance"]["value"],
+        "ratio_vs_sequential": s["speedup_vs_sequential"], "steps": s["steps"],
+        "instances": s["config"]["instances"], "dof_total": s["config"]["dof_total"],
+        "tile_shape": s["config"]["tile_shape"], "grid": s["config"]["grid"],
+        "roofline": s["roofline"], "clocks": s["clocks"]})
+    a_adj = copy.copy(a)
+    a_adj.steps = min(a.steps, 3)
+    a_adj.warmup = 1
+    timed("adjoint", lambda _a, c, p: run_adjoint(a_adj, c, p), lambda j: {
+        "forward_ms": j["forward_s"] * 1e3, "vjp_ms": j["vjp_s"] * 1e3,
+        "vjp_over_forward": j["vjp_over_forward"], "fd_check": j["fd_check"],
+        "steps": j["steps"], "timing": j["timing"]})
+    return out

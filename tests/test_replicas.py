@@ -84,3 +84,16 @@ def test_reference_arm_other_ranks_do_nothing(monkeypatch, capsys):
     monkeypatch.setenv("RANK", "1")
     bench.run_reference(argparse.Namespace(ref_device="cpu", steps=1, warmup=3, gpus=2))
     assert capsys.readouterr().out == ""
+
+
+def test_cpu_baseline_loop_times_the_adaptive_loop():
+    """The CPU baseline's loop leg runs the reference's integrateAdaptive (the compiled
+    reference where it was built, else the oracle port) on a row strip of the
+    configuration-2 mesh and reports DOF-updates/s over every right-hand side it took."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    r = bench.cpu_baseline_loop(None, rows=2, span=0.2)
+    assert r["value"] > 0 and r["cores"] == 1 and r["unit"] == bench.UNIT
+    assert r["kind"] in ("reference", "port")
+    assert "accepted" in r["sample"] and "2048x2" in r["sample"]
