@@ -323,7 +323,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   const bool wallL = C.bcx && ex0 == 0, wallR = C.bcx && ex0 + TXv == Nx;
   const bool wallB = C.bcy && ey0 == 0, wallT = C.bcy && ey0 + TYv == Ny;
 
-  long long gof[NIT];
+  int gof[NIT];  // node offset within one field (Nd <= 2^31 by the mesh-size limit)
   int sof[NIT];
   bool okk[NIT];
   auto item_map = [&]() {
@@ -332,7 +332,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       const int q = tid + NTHR * u;
       const int iy = q / RUN, k = q - iy * RUN;
       okk[u] = FULL || (iy < TYv && k < TXv * NPP);
-      gof[u] = ((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k;
+      gof[u] = (int)(((long long)ex0 + (long long)Nx * (ey0 + iy)) * NPP + k);
       sof[u] = iy * RUN + k;
     }
   };
@@ -356,7 +356,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           if (okk[u] && SGNB_INB(gof[u], Nd)) {
             const unsigned sa = (unsigned)__cvta_generic_to_shared(&(&S.G[v][0][0])[sof[u]]);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
-                         "l"(I.k + (long long)v * Nd + gof[u]) : "memory");
+                         "l"((I.k + (long long)v * Nd) + gof[u]) : "memory");
           }
     }
     // end-point stage: k1 and k2 by asynchronous copies into the (still unused) G, q and d
@@ -379,7 +379,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
             if (okk[u] && SGNB_INB(gof[u], Nd)) {
               const unsigned sa = (unsigned)__cvta_generic_to_shared(k12_slot(w, v) + sof[u]);
               asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
-                           "l"((w == 0 ? I.k1 : I.k2) + (long long)v * Nd + gof[u]) : "memory");
+                           "l"(((w == 0 ? I.k1 : I.k2) + (long long)v * Nd) + gof[u]) : "memory");
             }
     }
     // every u load (and, at the end point, every k3 load) of the tile in flight before the
@@ -392,8 +392,8 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u] && SGNB_INB(gof[u], Nd)) {
-            ux[v][u] = I.u[(long long)v * Nd + gof[u]];
-            if constexpr (MODE == MODE_FSAL) k3x[v][u] = I.k3[(long long)v * Nd + gof[u]];
+            ux[v][u] = (I.u + (long long)v * Nd)[gof[u]];
+            if constexpr (MODE == MODE_FSAL) k3x[v][u] = (I.k3 + (long long)v * Nd)[gof[u]];
           }
       cp_async_wait_all();  // k (k1, k2) and the statics have landed
     }
@@ -422,7 +422,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
           else if (v < 3) (&S.d[v - 1][0][0])[sof[u]] = x[u];
           else (&S.q[v - 3][0][0])[sof[u]] = (float)x[u];
           if constexpr (MODE == MODE_FSAL)
-            if (SGNB_INB(gof[u], Nd)) __stcs(&unew[(long long)v * Nd + gof[u]], x[u]);
+            if (SGNB_INB(gof[u], Nd)) __stcs(&(unew + (long long)v * Nd)[gof[u]], x[u]);
         }
     }
     // halos
@@ -664,15 +664,15 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       for (int u = 0; u < NIT; ++u)
         if (okk[u] && SGNB_INB(gof[u], Nd)) {
           const float val = (&S.G[v][0][0])[sof[u]];
-          if (A.outd) __stcs(&A.outd[(long long)v * Nd + gof[u]], (double)val);
-          else __stcs(&A.out[(long long)v * Nd + gof[u]], val);
+          if (A.outd) __stcs(&(A.outd + (long long)v * Nd)[gof[u]], (double)val);
+          else __stcs(&(A.out + (long long)v * Nd)[gof[u]], val);
         }
   } else if constexpr (MODE == MODE_STAGE) {
 #pragma unroll 1
     for (int v = 0; v < NV; ++v)
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
-        if (okk[u] && SGNB_INB(gof[u], Nd)) __stcs(&A.out[(long long)v * Nd + gof[u]], (&S.G[v][0][0])[sof[u]]);
+        if (okk[u] && SGNB_INB(gof[u], Nd)) __stcs(&(A.out + (long long)v * Nd)[gof[u]], (&S.G[v][0][0])[sof[u]]);
   } else {
     const volatile CtrlState* vc = A.ctrl;
     cur = vc->cur;
@@ -690,7 +690,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
     for (int u = 0; u < NIT; ++u)
       if (okk[u]) {
-        const long long g = gof[u];
+        const int g = gof[u];
         if (SGNB_INB(g, Nd)) { uu[u] = __ldcs(&u0[g]); c1[u] = __ldcs(&k1p[g]); c2[u] = __ldcs(&k2p[g]); c3[u] = __ldcs(&k3p[g]); }
       }
 #pragma unroll 1
@@ -699,15 +699,16 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
 #pragma unroll
         for (int u = 0; u < NIT; ++u)
           if (okk[u]) {
-            const long long g = (long long)(v + 1) * Nd + gof[u];
-            if (SGNB_INB(g, NV * Nd)) { nu[u] = __ldcs(&u0[g]); n1[u] = __ldcs(&k1p[g]); n2[u] = __ldcs(&k2p[g]); n3[u] = __ldcs(&k3p[g]); }
+            const long long o = (long long)(v + 1) * Nd;
+            const int gi = gof[u];
+            if (SGNB_INB(o + gi, NV * Nd)) { nu[u] = __ldcs(&(u0 + o)[gi]); n1[u] = __ldcs(&(k1p + o)[gi]); n2[u] = __ldcs(&(k2p + o)[gi]); n3[u] = __ldcs(&(k3p + o)[gi]); }
           }
       }
 #pragma unroll
       for (int u = 0; u < NIT; ++u)
         if (okk[u]) {
           const float k4 = (&S.G[v][0][0])[sof[u]];
-          if (SGNB_INB(gof[u], Nd)) __stcs(&outp[(long long)v * Nd + gof[u]], k4);
+          if (SGNB_INB(gof[u], Nd)) __stcs(&(outp + (long long)v * Nd)[gof[u]], k4);
           const double b1 = c1[u], b2 = c2[u], b3 = c3[u], b4 = k4;
           const double un = uu[u] + dt * (2.0 / 9.0 * b1 + 1.0 / 3.0 * b2 + 4.0 / 9.0 * b3);
           const double uEmb = uu[u] + dt * (7.0 / 24.0 * b1 + 0.25 * b2 + 1.0 / 3.0 * b3 + 0.125 * b4);
