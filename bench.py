@@ -24,6 +24,8 @@ contexts (--no-extras skips them):
                  sha256 with the fast mode's relative difference;
   batched        configuration 4's 256-instance sweep, batched against the same instances
                  run one after another;
+  batched_mixed  the same sweep in the mixed-precision mode, against the sequential FP64
+                 runs of the batched record and the sequential mixed ones;
   adjoint        configuration 5's forward and VJP times and a central-difference check;
   reference_gpu  the reference's own single-GPU solver (SGN2DCuda::integrateAdaptive,
                  oracle/_ref/ref_gpu_bench) on configuration 2 with periodic boundaries.

@@ -440,6 +440,18 @@ def default_extras(args, clock_sampler, peak):
         "instances": s["config"]["instances"], "dof_total": s["config"]["dof_total"],
         "tile_shape": s["config"]["tile_shape"], "grid": s["config"]["grid"],
         "roofline": s["roofline"], "clocks": s["clocks"]})
+    # the same sweep in mixed precision, against the same instances run one after another
+    # in plain FP64 (the batched record's sequential runs) and in mixed precision
+    a_mix = copy.copy(a)
+    a_mix.precision = "mixed"
+    seq64 = out["batched"].get("sequential_value")
+    timed("batched_mixed", lambda _a, c, p: run_sweep(a_mix, c, p), lambda s: {
+        "value": s["value"], "sequential_fp64_value": seq64,
+        "ratio_vs_sequential_fp64": s["value"] / seq64 if seq64 else None,
+        "sequential_mixed_value": s["sequential_single_instance"]["value"],
+        "ratio_vs_sequential_mixed": s["speedup_vs_sequential"], "steps": s["steps"],
+        "tile_shape": s["config"]["tile_shape"], "grid": s["config"]["grid"],
+        "roofline": s["roofline"], "clocks": s["clocks"]})
     a_adj = copy.copy(a)
     a_adj.steps = min(a.steps, 3)
     a_adj.warmup = 1
