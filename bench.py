@@ -20,12 +20,15 @@ runs independent replicas, one per GPU (the path does not exchange data between
 instances). At N = 1 the line also carries, each measured after the main run on its own
 contexts (--no-extras skips them):
   mixed          configuration 2 in the mixed-precision mode against FP64 in the same run,
-                 the eta errors of both step sequences, and the exact mode's final-state
-                 sha256 with the fast mode's relative difference;
+                 the eta errors of both step sequences, the exact mode's final-state
+                 sha256 with the fast mode's relative difference, and each mode's
+                 throughput on the frozen replay of the FP64 run's steps;
   batched        configuration 4's 256-instance sweep, batched against the same instances
                  run one after another;
   batched_mixed  the same sweep in the mixed-precision mode, against the sequential FP64
                  runs of the batched record and the sequential mixed ones;
+  slabs          configuration 2 on 4 x slabs of one device (edge copies between the slabs,
+                 and the fused exchange) against the whole-mesh loop;
   adjoint        configuration 5's forward and VJP times and a central-difference check;
   reference_gpu  the reference's own single-GPU solver (SGN2DCuda::integrateAdaptive,
                  oracle/_ref/ref_gpu_bench) on configuration 2 with periodic boundaries.

@@ -24,10 +24,15 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
     if (ghost) k_fused<MODE, SGNB_EXACT, true, true><<<grid, NTHR, smem, s>>>(C, A);
     else k_fused<MODE, SGNB_EXACT, true, false><<<grid, NTHR, smem, s>>>(C, A);
   } else {
-    if (ghost) k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
-    else if (C.Nx % 8 == 0 && C.Ny % 4 == 0)  // every tile full
+    const bool full = C.Nx % 8 == 0 && C.Ny % 4 == 0;  // every tile full
+    if (ghost) {
+      if (full) k_fused<MODE, SGNB_EXACT, false, true, false, true><<<grid, NTHR, smem, s>>>(C, A);
+      else k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
+    } else if (full) {
       k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
-    else k_fused<MODE, SGNB_EXACT, false, false><<<grid, NTHR, smem, s>>>(C, A);
+    } else {
+      k_fused<MODE, SGNB_EXACT, false, false><<<grid, NTHR, smem, s>>>(C, A);
+    }
   }
   return cudaGetLastError();
 }
@@ -54,6 +59,7 @@ static cudaError_t prepare_all() {
   if (e == cudaSuccess) e = prepare_variant<false, false, true>();
   if (e == cudaSuccess) e = prepare_variant<true, false, true>();
   if (e == cudaSuccess) e = prepare_variant<false, false, false, true>();
+  if (e == cudaSuccess) e = prepare_variant<false, true, false, true>();
   return e;
 }
 

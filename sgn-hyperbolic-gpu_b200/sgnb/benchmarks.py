@@ -1,7 +1,7 @@
 """Measurements of the batched sweep, the mixed-precision form and the adjoint, each
 returning one JSON line in the format of bench.py (which prints it for --workload
-sweep | mixed | adjoint | slabs, and folds a summary of the first three into its default
-line through default_extras). Every number is taken on the device with CUDA events on the
+sweep | mixed | adjoint | slabs, and folds summaries of all four into its default line
+through default_extras). Every number is taken on the device with CUDA events on the
 stream the work runs on, after warm-up, with the state resident in HBM.
 
 sweep    configuration 4: 256 instances (workloads.cfg4_instances) advanced K accepted
@@ -148,6 +148,7 @@ def run_mixed(args, clock_sampler, peak):
     seqs = {}
     finals = {"adaptive": {}, "stable": {}}
     full = {}
+    replay = {}
     clocks = None
     for name, prec in (("fp64", FP64_FAST), ("mixed", MIXED), ("exact", FP64_EXACT)):
         with SGN2DB200(precision=prec, **kw) as d:
@@ -174,11 +175,23 @@ def run_mixed(args, clock_sampler, peak):
                 log = d.attempt_log()
                 seqs["adaptive"] = log[log[:, 3] == 1][:, 1].copy()
                 seqs["stable"] = np.full(len(seqs["adaptive"]), 0.4 * dt0)
-            # free surface after each step sequence, from the same state
-            for key, dts in seqs.items():
+            # free surface after each step sequence, from the same state (the adaptive
+            # sequence's replay timed, after the stable one has warmed the kernels up: the
+            # exact mode's throughput beside the fast one's)
+            for key in ("stable", "adaptive"):
+                dts = seqs[key]
                 d.upload_tensor(Ud)
                 try:
+                    _, sp = d.state_device_ptr()
+                    stream = torch.cuda.ExternalStream(sp)
+                    e0, e1 = _events(torch, stream)
+                    torch.cuda.synchronize()
+                    e0.record(stream)
                     d.bs3_steps(0.0, dts)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    if key == "adaptive":
+                        replay[name] = dof * 3 * len(dts) / (e0.elapsed_time(e1) / 1e3)
                     finals[key][name] = d.state_tensor()[: d.Nd].clone()  # h
                     if key == "adaptive" and name in ("fp64", "exact"):
                         full[name] = d.state_tensor().clone()
@@ -222,6 +235,8 @@ def run_mixed(args, clock_sampler, peak):
         "config": {"workload": f"configuration 2 ({Nx}x{Ny}, {int(dof):,} DOF), mixed "
                                "precision against FP64 (fast)", "mesh": [Nx, Ny]},
         "fp64": res["fp64"], "mixed": res["mixed"], "speedup_vs_fp64": ratio,
+        "replay_value": {"how": "the FP64 run's accepted step sizes replayed as frozen BS3 "
+                                "steps (3 right-hand sides each), CUDA events", **replay},
         "eta_error": errors,
         "roofline": {"bound": "hbm", "kernel": "mixed stage loop (average over an attempt)",
                      "achieved": round(achieved, 1), "peak": peak[0], "peak_kind": peak[1],
@@ -303,7 +318,8 @@ def run_adjoint(args, clock_sampler, peak):
     return line
 
 
-def run_slabs(args, clock_sampler, peak):
+def run_slabs(args, clock_sampler, peak, counts=(1, 2, 4),
+              fused_runs=((2, "per-slab"), (2, "shared"), (4, "per-slab"), (4, "shared"))):
     """Configuration 2 on x slabs of one device (1, 2 and 4 slabs: the edge exchange and
     the partial gather between slabs are device copies on the solver's stream, every
     stage launched from the host), against the whole-mesh device loop: K accepted steps
@@ -347,7 +363,7 @@ def run_slabs(args, clock_sampler, peak):
         ref = d.state_tensor().clone()
     slabs = {}
     clocks = None
-    for n in (1, 2, 4):
+    for n in counts:
         with SlabSolver(kw, nslabs=n) as s:
             s.upload_tensor(Ud)
             s.integrate_steps(0.0, dt0, args.warmup)
@@ -367,33 +383,34 @@ def run_slabs(args, clock_sampler, peak):
     # the fused edge exchange: stage kernels store the neighbours' ghosts, controllers read
     # every slab's partials in place; one stream per slab (ordered by events) or one shared
     fused = {}
-    for n in (2, 4):
-        for mode in ("per-slab", "shared"):
-            with PeerSlabSolver(kw, nslabs=n, streams=mode) as s:
-                s.upload_tensor(Ud)
-                s.integrate_steps(0.0, dt0, args.warmup)
-                s.upload_tensor(Ud)
-                e0, e1 = _events(torch, s.stream)
-                torch.cuda.synchronize()
-                e0.record(s.stream)
-                st = s.integrate_steps(0.0, dt0, args.steps)
-                e1.record(s.stream)
-                torch.cuda.synchronize()
-                t = e0.elapsed_time(e1) / 1e3
-                fused[f"{n} {mode}"] = dict(value=dof * st.rhsEvals / t,
-                                           ms_per_step=t / args.steps * 1e3,
-                                           accepted=st.accepted, rejected=st.rejected,
-                                           rel_diff_vs_whole=rel(s.download_tensor(), ref))
-    top = slabs["4"]
+    for n, mode in fused_runs:
+        with PeerSlabSolver(kw, nslabs=n, streams=mode) as s:
+            s.upload_tensor(Ud)
+            s.integrate_steps(0.0, dt0, args.warmup)
+            s.upload_tensor(Ud)
+            e0, e1 = _events(torch, s.stream)
+            torch.cuda.synchronize()
+            e0.record(s.stream)
+            st = s.integrate_steps(0.0, dt0, args.steps)
+            e1.record(s.stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            fused[f"{n} {mode}"] = dict(value=dof * st.rhsEvals / t,
+                                       ms_per_step=t / args.steps * 1e3,
+                                       accepted=st.accepted, rejected=st.rejected,
+                                       rel_diff_vs_whole=rel(s.download_tensor(), ref))
+    nmax = max(counts)
+    top = slabs[str(nmax)]
     edge_bytes = 5 * Ny * 5 * 8
     line = {
         "metric": METRIC, "value": top["value"], "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": top["ms_per_step"],
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"configuration 2 ({Nx}x{Ny}, walls, adaptive BS3(2)) on 4 x "
-                               "slabs of one device; the whole-mesh loop and 1 and 2 slabs "
-                               "beside it",
+        "config": {"workload": f"configuration 2 ({Nx}x{Ny}, walls, adaptive BS3(2)) on "
+                               f"{nmax} x slabs of one device; the whole-mesh loop and "
+                               f"{', '.join(str(n) for n in counts if n != nmax) or 'no other'} "
+                               "slab counts beside it",
                    "edge_bytes": edge_bytes,
                    "exchange_bytes_per_attempt_per_slab": 3 * 2 * edge_bytes,
                    "l2": f"inputs larger than L2 ({8 * 5 * dof / 1e9:.1f} GB per state)"},
@@ -433,6 +450,7 @@ def default_extras(args, clock_sampler, peak):
     timed("mixed", run_mixed, lambda m: {
         "value": m["value"], "fp64_value_same_run": m["fp64"]["value"],
         "ratio_vs_fp64": m["speedup_vs_fp64"], "steps": m["steps"],
+        "replay_value": m["replay_value"],
         "eta_error": m["eta_error"], "roofline": m["roofline"], "clocks": m["clocks"]})
     timed("batched", run_sweep, lambda s: {
         "value": s["value"], "sequential_value": s["sequential_single_instance"]["value"],
@@ -452,6 +470,12 @@ def default_extras(args, clock_sampler, peak):
         "ratio_vs_sequential_mixed": s["speedup_vs_sequential"], "steps": s["steps"],
         "tile_shape": s["config"]["tile_shape"], "grid": s["config"]["grid"],
         "roofline": s["roofline"], "clocks": s["clocks"]})
+    # x slabs of one device: 4 slabs with copies between them and with the fused exchange
+    timed("slabs", lambda _a, c, p: run_slabs(_a, c, p, counts=(4,), fused_runs=((4, "per-slab"),)),
+          lambda s: {"whole_mesh": s["whole_mesh"], "slabs": s["slabs"],
+                     "fused_exchange": s["fused_exchange"],
+                     "slab_over_whole": s["slab_over_whole"], "clocks": s["clocks"],
+                     "timing": s["timing"]})
     a_adj = copy.copy(a)
     a_adj.steps = min(a.steps, 3)
     a_adj.warmup = 1
