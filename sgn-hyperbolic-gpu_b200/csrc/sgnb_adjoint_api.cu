@@ -63,8 +63,11 @@ int afail(sgnb_ctx* c, int code, const std::string& m) {
 
 FrTablesDev tables_of(const sgnb_ctx* c) {
   FrTablesDev T{};
-  for (int k = 0; k < 25; ++k) T.D[k] = c->tab.D[k];
-  for (int k = 0; k < 5; ++k) { T.gLp[k] = c->tab.gLp[k]; T.gRp[k] = c->tab.gRp[k]; }
+  for (int k = 0; k < 25; ++k) { T.D[k] = c->tab.D[k]; T.Df[k] = (float)c->tab.D[k]; }
+  for (int k = 0; k < 5; ++k) {
+    T.gLp[k] = c->tab.gLp[k]; T.gRp[k] = c->tab.gRp[k];
+    T.gLpf[k] = (float)c->tab.gLp[k]; T.gRpf[k] = (float)c->tab.gRp[k];
+  }
   return T;
 }
 

@@ -192,10 +192,15 @@ void fill_consts(sgnb_ctx* c) {
   C.Jy = 0.5 * c->mesh.hy;
   C.iJx = 1.0 / C.Jx;
   C.iJy = 1.0 / C.Jy;
-  for (int k = 0; k < 25; ++k) C.D[k] = c->tab.D[k];
+  for (int k = 0; k < 25; ++k) {
+    C.D[k] = c->tab.D[k];
+    C.Df[k] = (float)c->tab.D[k];
+  }
   for (int k = 0; k < 5; ++k) {
     C.gLp[k] = c->tab.gLp[k];
     C.gRp[k] = c->tab.gRp[k];
+    C.gLpf[k] = (float)c->tab.gLp[k];
+    C.gRpf[k] = (float)c->tab.gRp[k];
     C.lL[k] = c->tab.lL[k];
     C.lR[k] = c->tab.lR[k];
   }
@@ -863,8 +868,11 @@ cudaError_t batch_launch(sgnb_batch* b, int mode, int shape, int blocks, int kin
 BatchArgs batch_args(sgnb_batch* b, int shape, int kin_k2, double coef) {
   BatchArgs B{};
   const RhsConsts& C0 = b->ctx[0]->C;
-  for (int k = 0; k < 25; ++k) B.tables.D[k] = C0.D[k];
-  for (int k = 0; k < 5; ++k) { B.tables.gLp[k] = C0.gLp[k]; B.tables.gRp[k] = C0.gRp[k]; }
+  for (int k = 0; k < 25; ++k) { B.tables.D[k] = C0.D[k]; B.tables.Df[k] = C0.Df[k]; }
+  for (int k = 0; k < 5; ++k) {
+    B.tables.gLp[k] = C0.gLp[k]; B.tables.gRp[k] = C0.gRp[k];
+    B.tables.gLpf[k] = C0.gLpf[k]; B.tables.gRpf[k] = C0.gRpf[k];
+  }
   B.consts = b->dconsts;
   B.args = b->dargs;
   B.tile_inst = b->dtile_inst[shape];

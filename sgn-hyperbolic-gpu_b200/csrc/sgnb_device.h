@@ -50,6 +50,9 @@ struct RhsConsts {
   double* tr;
   int gauss;
   int pad2_;
+  // the differentiation and correction tables rounded to FP32 (the mixed mode's FP32
+  // contractions)
+  float Df[25], gLpf[5], gRpf[5];
 };
 
 // Device-resident state of the adaptive integrator: the scalar loop variables of
@@ -70,6 +73,27 @@ struct CtrlState {
   long long maxAccepted; // > 0: stop after this many accepted steps
   long long attemptCap;  // the device-side loop hands back to the host at this attempt count
 };
+
+#ifdef __CUDACC__
+// The controller's per-launch values (buffer index, dt, tolerances) read again late in a
+// stage kernel, through the read-only path: the controller state does not change while a
+// stage kernel runs (the controller kernel writes it between launches), so after the
+// first read on an SM the line comes from L1 instead of an L2 round trip. Asm statements,
+// so the compiler neither merges them with the kernel's first read nor keeps that value
+// live in registers in between.
+struct CtrlReload {
+  int cur;
+  double dt, atol, rtol;
+};
+__device__ __forceinline__ CtrlReload ctrl_reload(const CtrlState* c) {
+  CtrlReload r;
+  asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(r.cur) : "l"(&c->cur));
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(r.dt) : "l"(&c->dt));
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(r.atol) : "l"(&c->atol));
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(r.rtol) : "l"(&c->rtol));
+  return r;
+}
+#endif
 
 // Buffers of one fused launch.
 struct StageArgs {
@@ -104,6 +128,7 @@ struct StageArgsM {
 // instance's local tile t - tile_start[inst]; per-instance constants and buffers.
 struct FrTablesDev {
   double D[25], gLp[5], gRp[5];
+  float Df[25], gLpf[5], gRpf[5];  // FP32 roundings (mixed mode)
 };
 
 struct BatchArgs {
