@@ -486,11 +486,11 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
 
   // ---- own-node item map: NIT items per thread, shared by every array -------
   // item u of a thread is double k of tile row iy: global (e_row*25 + k), shared
-  // iy*RUN + k (the [TE][NPP] layout of one field). The stage modes keep a thread's items
-  // in one tile row, NTHR / TY doubles apart (one base address and immediate offsets: the
-  // end-point stage 1.3 % faster); the rhs-only mode takes q = tid + NTHR*u in tile-row
-  // order (1 % faster there). Recomputed after the passes rather than kept live through
-  // them.
+  // iy*RUN + k (the [TE][NPP] layout of one field). The stage modes on full tiles keep a
+  // thread's items in one tile row, NTHR / TY doubles apart (one base address and
+  // immediate offsets: the end-point stage 1.3 % faster); the rhs-only mode and partial
+  // tiles (the batched kernels) take q = tid + NTHR*u in tile-row order (1 % and 0.3 %
+  // faster there). Recomputed after the passes rather than kept live through them.
   int gof[NIT];  // node offset within one field (Nd <= 2^31 by the mesh-size limit)
   int sof[NIT];
   bool okk[NIT];
@@ -500,7 +500,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
       constexpr int PER_ROW = NTHR / TY;
       static_assert(NTHR % TY == 0 && RUN == NIT * PER_ROW, "items split evenly over the rows");
       int iy, k;
-      if constexpr (MODE != MODE_RHS) {
+      if constexpr (MODE != MODE_RHS && FULL) {
         iy = tid / PER_ROW;
         k = tid - iy * PER_ROW + PER_ROW * u;
       } else {

@@ -329,13 +329,14 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   auto item_map = [&]() {
 #pragma unroll
     for (int u = 0; u < NIT; ++u) {
-      // the end-point stage keeps a thread's items in one tile row, NTHR / TY doubles
-      // apart (one base address and immediate offsets: 1.1 % faster); the other modes take
-      // q = tid + NTHR*u in tile-row order
+      // the end-point stage on full tiles keeps a thread's items in one tile row, NTHR /
+      // TY doubles apart (one base address and immediate offsets: 1.1 % faster); the other
+      // modes and partial tiles (the batched kernel, 0.9 % faster so) take q = tid + NTHR*u
+      // in tile-row order
       constexpr int PER_ROW = NTHR / TY;
       static_assert(NTHR % TY == 0 && RUN == NIT * PER_ROW, "items split evenly over the rows");
       int iy, k;
-      if constexpr (MODE == MODE_FSAL) {
+      if constexpr (MODE == MODE_FSAL && FULL) {
         iy = tid / PER_ROW;
         k = tid - iy * PER_ROW + PER_ROW * u;
       } else {
