@@ -251,6 +251,14 @@ def run_ours(args):
                 "traffic": (round(traffic * dof) if traffic else None),
                 "algorithmic_bytes": round(bpd[dominant] * dof),
                 "launch_ms": {k: round(v * 1e3, 4) for k, v in per.items()}}
+    # both stage kernels, with their shares of an attempt (two intermediate stages and one
+    # end point): the two are close to even, so the dominant one can change between runs
+    attempt = 2 * per["stage"] + per["fsal"]
+    roofline["kernels"] = {
+        k: {"achieved": round(bpd[k] * dof / per[k] / 1e9, 1),
+            "frac": round(bpd[k] * dof / per[k] / 1e9 / peak, 4),
+            "share_of_attempt": round((2 if k == "stage" else 1) * per[k] / attempt, 4)}
+        for k in ("stage", "fsal")}
 
     # ---- e2e through the public API with host buffers ----------------------------
     torch.cuda.synchronize()
