@@ -93,6 +93,29 @@ __device__ __forceinline__ CtrlReload ctrl_reload(const CtrlState* c) {
   asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(r.rtol) : "l"(&c->rtol));
   return r;
 }
+
+// Block-wide copy of two parameter blocks (W1 and W2 32-bit words) from global to shared
+// memory, by NT threads: every load of a thread is issued before its first store, so the
+// copy costs one memory round trip however many words a thread moves.
+template <int W1, int W2, int NT>
+__device__ __forceinline__ void block_copy2(unsigned* d1, const unsigned* s1, unsigned* d2,
+                                            const unsigned* s2) {
+  constexpr int R1 = (W1 + NT - 1) / NT, R2 = (W2 + NT - 1) / NT;
+  unsigned t1[R1], t2[R2];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < R1; ++r)
+    if (tid + r * NT < W1) t1[r] = s1[tid + r * NT];
+#pragma unroll
+  for (int r = 0; r < R2; ++r)
+    if (tid + r * NT < W2) t2[r] = s2[tid + r * NT];
+#pragma unroll
+  for (int r = 0; r < R1; ++r)
+    if (tid + r * NT < W1) d1[tid + r * NT] = t1[r];
+#pragma unroll
+  for (int r = 0; r < R2; ++r)
+    if (tid + r * NT < W2) d2[tid + r * NT] = t2[r];
+}
 #endif
 
 // Buffers of one fused launch.

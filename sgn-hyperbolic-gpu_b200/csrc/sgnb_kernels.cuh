@@ -1070,12 +1070,10 @@ __device__ __forceinline__ void batch_tile(const BatchArgs& B, long long t,
   const long long lt = t - B.tile_start[inst];
   __syncthreads();  // the previous tile is done with Cs / As
   {
-    const unsigned* src = reinterpret_cast<const unsigned*>(B.consts + inst);
-    unsigned* dst = reinterpret_cast<unsigned*>(&Cs);
-    for (int w = threadIdx.x; w < (int)(sizeof(RhsConsts) / 4); w += NTHR) dst[w] = src[w];
-    const unsigned* srca = reinterpret_cast<const unsigned*>(B.args + inst);
-    unsigned* dsta = reinterpret_cast<unsigned*>(&As);
-    for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 4); w += NTHR) dsta[w] = srca[w];
+    // both blocks' loads in flight before the first store (one round trip per tile)
+    block_copy2<(int)(sizeof(RhsConsts) / 4), (int)(sizeof(StageArgs) / 4), NTHR>(
+        reinterpret_cast<unsigned*>(&Cs), reinterpret_cast<const unsigned*>(B.consts + inst),
+        reinterpret_cast<unsigned*>(&As), reinterpret_cast<const unsigned*>(B.args + inst));
   }
   __syncthreads();
   if (threadIdx.x == 0) {

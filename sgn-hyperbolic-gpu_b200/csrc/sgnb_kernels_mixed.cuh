@@ -359,6 +359,127 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       if (okk[u]) {
         if (SGNB_INB(gof[u], Nd)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
       }
+    // halos: the neighbour tiles' trace nodes, stage inputs formed in registers
+    double hv[NHIT];
+    int hq[NHIT];
+    auto halo_load = [&]() {
+      long long hg[NHIT];
+#pragma unroll
+      for (int u = 0; u < NHIT; ++u) {
+        const int q = tid + NTHR * u;
+        const int t = q % NP, r = q / NP;
+        const int slot = r % NHALO, v = r / NHALO;
+        bool ok = q < NV * NHALO * NP;
+        long long e = 0;
+        int node = 0;
+        if (slot < TY) {
+          ok = ok && slot < TYv && !wallL;
+          e = (long long)(exL) + (long long)Nx * (ey0 + slot);
+          node = (NP - 1) + NP * t;
+        } else if (slot < 2 * TY) {
+          ok = ok && slot - TY < TYv && !wallR;
+          e = (long long)(exR) + (long long)Nx * (ey0 + slot - TY);
+          node = NP * t;
+        } else if (slot < 2 * TY + TX) {
+          ok = ok && slot - 2 * TY < TXv && !wallB;
+          e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * (eyB);
+          node = t + NP * (NP - 1);
+        } else {
+          ok = ok && slot - 2 * TY - TX < TXv && !wallT;
+          e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * (eyT);
+          node = t;
+        }
+        hq[u] = ok ? q : -1;
+        hg[u] = (long long)v * Nd + e * NPP + node;
+      }
+#pragma unroll
+      for (int u = 0; u < NHIT; ++u)
+        if (hq[u] >= 0 && SGNB_INB(hg[u], NV * Nd)) hv[u] = stage_value<MODE>(I, hg[u]);
+    };
+    // face depths through registers (right-hand-side mode)
+    auto face_load = [&](double (&fv)[NFIT], int (&fq)[NFIT]) {
+#pragma unroll
+      for (int u = 0; u < NFIT; ++u) {
+        const int q = tid + NTHR * u;
+        fq[u] = -1;
+        if (q < 2 * TE * NP) {
+          const int t = q % NP, i = (q / NP) % TE, s = q / (NP * TE);
+          const int ix = i % TX, iy = i / TX;
+          if (ix < TXv && iy < TYv) {
+            const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
+            fv[u] = SGNB_INB(e * NP + t, Nd / NP) ? (s == 0 ? C.HfX : C.HfY)[e * NP + t] : 0.0;
+            fq[u] = q;
+          }
+        } else if (q < NFACE) {
+          const int r = q - 2 * TE * NP;
+          const int t = r % NP, slot = r / NP;
+          if (slot < TY) {
+            if (slot < TYv) {
+              const int ey = ey0 + slot;
+              fv[u] = SGNB_INB(wallR ? (long long)ey * NP + t
+                                     : ((long long)(exR) + (long long)Nx * ey) * NP + t,
+                               wallR ? (long long)Ny * NP : Nd / NP)
+                          ? (wallR ? C.HfXEnd[(long long)ey * NP + t]
+                            : C.HfX[((long long)(exR) + (long long)Nx * ey) * NP + t])
+                          : 0.0;
+              fq[u] = q;
+            }
+          } else if (slot - TY < TXv) {
+            const int ex = ex0 + slot - TY;
+            fv[u] = SGNB_INB(wallT ? (long long)ex * NP + t
+                                   : ((long long)ex + (long long)Nx * (eyT)) * NP + t,
+                             wallT ? (long long)Nx * NP : Nd / NP)
+                        ? (wallT ? C.HfYEnd[(long long)ex * NP + t]
+                          : C.HfY[((long long)ex + (long long)Nx * (eyT)) * NP + t])
+                        : 0.0;
+            fq[u] = q;
+          }
+        }
+      }
+    };
+    // stage modes: face depths by asynchronous copies straight into shared memory, issued
+    // with the statics (the right-hand-side mode is faster loading them after its state)
+    if constexpr (MODE != MODE_RHS) {
+#pragma unroll
+      for (int u = 0; u < NFIT; ++u) {
+        const int q = tid + NTHR * u;
+        const double* fp = nullptr;  // source of face-depth item q (none: not in this tile)
+        bool fok = false;
+        if (q < 2 * TE * NP) {
+          const int t = q % NP, i = (q / NP) % TE, s = q / (NP * TE);
+          const int ix = i % TX, iy = i / TX;
+          if (ix < TXv && iy < TYv) {
+            const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
+            fok = true;
+            if (SGNB_INB(e * NP + t, Nd / NP)) fp = (s == 0 ? C.HfX : C.HfY) + e * NP + t;
+          }
+        } else if (q < NFACE) {
+          const int r = q - 2 * TE * NP;
+          const int t = r % NP, slot = r / NP;
+          if (slot < TY) {
+            if (slot < TYv) {
+              const int ey = ey0 + slot;
+              const long long fe = (long long)ey * NP + t;
+              const long long fx = ((long long)(exR) + (long long)Nx * ey) * NP + t;
+              fok = true;
+              if (wallR) { if (SGNB_INB(fe, (long long)Ny * NP)) fp = C.HfXEnd + fe; }
+              else if (SGNB_INB(fx, Nd / NP)) fp = C.HfX + fx;
+            }
+          } else if (slot - TY < TXv) {
+            const int ex = ex0 + slot - TY;
+            const long long fe = (long long)ex * NP + t;
+            const long long fy = ((long long)ex + (long long)Nx * (eyT)) * NP + t;
+            fok = true;
+            if (wallT) { if (SGNB_INB(fe, (long long)Nx * NP)) fp = C.HfYEnd + fe; }
+            else if (SGNB_INB(fy, Nd / NP)) fp = C.HfY + fy;
+          }
+        }
+        if (fok && SGNB_INB(q, NFACE)) {
+          if (fp) cp_async8(&S.Hf[q], fp);
+          else S.Hf[q] = 0.0;
+        }
+      }
+    }
     double* __restrict__ unew = A.U[cur ^ 1];
     if constexpr (MODE == MODE_STAGE) {
       // k (FP32) by asynchronous copies into the still unused G area
@@ -395,6 +516,9 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
                            "l"(((w == 0 ? I.k1 : I.k2) + (long long)v * Nd) + gof[u]) : "memory");
             }
     }
+    // end-point stage: the halo loads go first, in flight together with the tile's own
+    // (the other modes are faster issuing them after the combination)
+    if constexpr (MODE == MODE_FSAL) halo_load();
     // every u load (and, at the end point, every k3 load) of the tile in flight before the
     // first combination
     double ux[NV][NIT];
@@ -438,81 +562,10 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
             if (SGNB_INB(gof[u], Nd)) __stcs(&(unew + (long long)v * Nd)[gof[u]], x[u]);
         }
     }
-    // halos
-    double hv[NHIT];
-    int hq[NHIT];
-    long long hg[NHIT];
-#pragma unroll
-    for (int u = 0; u < NHIT; ++u) {
-      const int q = tid + NTHR * u;
-      const int t = q % NP, r = q / NP;
-      const int slot = r % NHALO, v = r / NHALO;
-      bool ok = q < NV * NHALO * NP;
-      long long e = 0;
-      int node = 0;
-      if (slot < TY) {
-        ok = ok && slot < TYv && !wallL;
-        e = (long long)(exL) + (long long)Nx * (ey0 + slot);
-        node = (NP - 1) + NP * t;
-      } else if (slot < 2 * TY) {
-        ok = ok && slot - TY < TYv && !wallR;
-        e = (long long)(exR) + (long long)Nx * (ey0 + slot - TY);
-        node = NP * t;
-      } else if (slot < 2 * TY + TX) {
-        ok = ok && slot - 2 * TY < TXv && !wallB;
-        e = (long long)(ex0 + slot - 2 * TY) + (long long)Nx * (eyB);
-        node = t + NP * (NP - 1);
-      } else {
-        ok = ok && slot - 2 * TY - TX < TXv && !wallT;
-        e = (long long)(ex0 + slot - 2 * TY - TX) + (long long)Nx * (eyT);
-        node = t;
-      }
-      hq[u] = ok ? q : -1;
-      hg[u] = (long long)v * Nd + e * NPP + node;
-    }
-#pragma unroll
-    for (int u = 0; u < NHIT; ++u)
-      if (hq[u] >= 0 && SGNB_INB(hg[u], NV * Nd)) hv[u] = stage_value<MODE>(I, hg[u]);
+    if constexpr (MODE != MODE_FSAL) halo_load();
     double fv[NFIT];
     int fq[NFIT];
-#pragma unroll
-    for (int u = 0; u < NFIT; ++u) {
-      const int q = tid + NTHR * u;
-      fq[u] = -1;
-      if (q < 2 * TE * NP) {
-        const int t = q % NP, i = (q / NP) % TE, s = q / (NP * TE);
-        const int ix = i % TX, iy = i / TX;
-        if (ix < TXv && iy < TYv) {
-          const long long e = (long long)(ex0 + ix) + (long long)Nx * (ey0 + iy);
-          fv[u] = SGNB_INB(e * NP + t, Nd / NP) ? (s == 0 ? C.HfX : C.HfY)[e * NP + t] : 0.0;
-          fq[u] = q;
-        }
-      } else if (q < NFACE) {
-        const int r = q - 2 * TE * NP;
-        const int t = r % NP, slot = r / NP;
-        if (slot < TY) {
-          if (slot < TYv) {
-            const int ey = ey0 + slot;
-            fv[u] = SGNB_INB(wallR ? (long long)ey * NP + t
-                                   : ((long long)(exR) + (long long)Nx * ey) * NP + t,
-                             wallR ? (long long)Ny * NP : Nd / NP)
-                        ? (wallR ? C.HfXEnd[(long long)ey * NP + t]
-                          : C.HfX[((long long)(exR) + (long long)Nx * ey) * NP + t])
-                        : 0.0;
-            fq[u] = q;
-          }
-        } else if (slot - TY < TXv) {
-          const int ex = ex0 + slot - TY;
-          fv[u] = SGNB_INB(wallT ? (long long)ex * NP + t
-                                 : ((long long)ex + (long long)Nx * (eyT)) * NP + t,
-                           wallT ? (long long)Nx * NP : Nd / NP)
-                      ? (wallT ? C.HfYEnd[(long long)ex * NP + t]
-                        : C.HfY[((long long)ex + (long long)Nx * (eyT)) * NP + t])
-                      : 0.0;
-          fq[u] = q;
-        }
-      }
-    }
+    if constexpr (MODE == MODE_RHS) face_load(fv, fq);
 #pragma unroll
     for (int u = 0; u < NHIT; ++u)
       if (hq[u] >= 0 && SGNB_INB(hq[u], NV * NHALO * NP)) {
@@ -521,9 +574,11 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
         if (v < 3) S.hhalo[v * NHALO * NP + rest] = hv[u];
         else S.qhalo[(v - 3) * NHALO * NP + rest] = (float)hv[u];
       }
+    if constexpr (MODE == MODE_RHS) {
 #pragma unroll
-    for (int u = 0; u < NFIT; ++u)
-      if (fq[u] >= 0 && SGNB_INB(fq[u], NFACE)) S.Hf[fq[u]] = fv[u];
+      for (int u = 0; u < NFIT; ++u)
+        if (fq[u] >= 0 && SGNB_INB(fq[u], NFACE)) S.Hf[fq[u]] = fv[u];
+    }
     cp_async_wait_all();
   }
   __syncthreads();
@@ -791,12 +846,10 @@ __device__ __forceinline__ void mixed_batch_tile(const BatchArgsM& B, long long 
   const long long lt = t - B.tile_start[inst];
   __syncthreads();  // the previous tile is done with Cs / As
   {
-    const unsigned* src = reinterpret_cast<const unsigned*>(B.consts + inst);
-    unsigned* dst = reinterpret_cast<unsigned*>(&Cs);
-    for (int w = threadIdx.x; w < (int)(sizeof(RhsConsts) / 4); w += NTHR) dst[w] = src[w];
-    const unsigned* srca = reinterpret_cast<const unsigned*>(B.args + inst);
-    unsigned* dsta = reinterpret_cast<unsigned*>(&As);
-    for (int w = threadIdx.x; w < (int)(sizeof(StageArgsM) / 4); w += NTHR) dsta[w] = srca[w];
+    // both blocks' loads in flight before the first store (one round trip per tile)
+    block_copy2<(int)(sizeof(RhsConsts) / 4), (int)(sizeof(StageArgsM) / 4), NTHR>(
+        reinterpret_cast<unsigned*>(&Cs), reinterpret_cast<const unsigned*>(B.consts + inst),
+        reinterpret_cast<unsigned*>(&As), reinterpret_cast<const unsigned*>(B.args + inst));
   }
   __syncthreads();
   if (threadIdx.x == 0) {
