@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -74,8 +75,9 @@ cudaError_t launch(sgnb_ctx* c, const Launch& L, cudaStream_t s) {
   A.kin_k2 = L.stage == 3;
   A.coef = L.stage == 3 ? 0.75 : 0.5;
   A.out = L.mode == 0 ? L.out : (L.stage == 3 ? A.K3 : A.K2);
-  return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(L.mode, c->C, A, s)
-                                        : dev::launch_fused_exact(L.mode, c->C, A, s);
+  const TileMaps* M = c->maps.ok ? &c->maps : nullptr;  // A names the context's buffers
+  return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(L.mode, c->C, A, s, M)
+                                        : dev::launch_fused_exact(L.mode, c->C, A, s, M);
 }
 
 Launch rhs_launch(const double* in, double* out) {
@@ -172,6 +174,54 @@ Mesh mesh_for(const sgnb_desc* d) {
   m.ex0 = d->Nx_global > 0 ? d->ex_offset : 0;
   m.wrapx = d->Nx_global > 0 && d->bc_x == SGNB_BC_PERIODIC && d->ex_offset + d->Nx == d->Nx_global;
   return m;
+}
+
+// Tensor maps of the context's buffers for the fused kernels' tile loads (meshes that are
+// a whole number of 8x4 tiles). The encoder comes from the driver through the runtime, so
+// the library links no driver library; without it (or on any encoding error), or with
+// SGNB_TMA=0 in the environment at creation, the kernels keep their per-thread
+// asynchronous copies (the same results bit for bit: data movement only).
+static void build_tile_maps(sgnb_ctx* c) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  c->maps.ok = 0;
+  if (c->mixed || c->desc.Nx % 8 != 0 || c->desc.Ny % 4 != 0) return;
+  const char* sw = std::getenv("SGNB_TMA");
+  if (sw && sw[0] == '0') return;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+  if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault,
+                                       &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || fn == nullptr) {
+    cudaGetLastError();
+    return;
+  }
+  const Encode enc = reinterpret_cast<Encode>(fn);
+  const cuuint64_t W = (cuuint64_t)c->desc.Nx * 25, H = (cuuint64_t)c->desc.Ny;
+  // [field][element row][Nx * 25 doubles], box [5][4][200]: one 8x4 tile of every field
+  const cuuint64_t dim3[3] = {W, H, 5};
+  const cuuint64_t stride3[2] = {W * sizeof(double), (cuuint64_t)c->Nd * sizeof(double)};
+  const cuuint32_t box3[3] = {200, 4, 5};
+  const cuuint32_t one[3] = {1, 1, 1};
+  auto map3 = [&](CUtensorMap* m, const void* p) {
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(p), dim3, stride3, box3,
+               one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+  };
+  const cuuint64_t dim2[2] = {W, H};
+  const cuuint64_t stride2[1] = {W * sizeof(double)};
+  const cuuint32_t box2[2] = {200, 4};
+  bool ok = map3(&c->maps.U[0], c->U[0]) && map3(&c->maps.U[1], c->U[1]) &&
+            map3(&c->maps.K1[0], c->K1[0]) && map3(&c->maps.K1[1], c->K1[1]) &&
+            map3(&c->maps.K2, c->K2) && map3(&c->maps.K3, c->K3);
+  ok = ok && enc(&c->maps.H, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(c->C.Hnod),
+                 dim2, stride2, box2, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  c->maps.ok = ok ? 1 : 0;
 }
 
 void fill_consts(sgnb_ctx* c) {
@@ -484,6 +534,7 @@ int sgnb_create(const sgnb_desc* d, sgnb_ctx** out) {
   e = cudaMalloc(&c->K2, 2 * kbytes);
   if (e != cudaSuccess) { cuda_fail(c, e, "cudaMalloc(stage)"); g_create_error = c->err; return bail(SGNB_ERR_NOMEM); }
   c->K3 = (char*)c->K2 + kbytes;
+  build_tile_maps(c);
   e = cudaMemset(c->U[0], 0, sbytes);
   c->nblk = dev::fused_grid_blocks(d->Nx, d->Ny);
   c->ndiag = 592;

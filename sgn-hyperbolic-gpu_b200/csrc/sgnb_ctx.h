@@ -20,6 +20,7 @@ struct sgnb_ctx {
   sgnb::FrTables tab;
   long long Nd = 0, ntot = 0;
   sgnb::RhsConsts C{};
+  sgnb::TileMaps maps{};  // tensor maps of U, K1, K2, K3, Hnod (FP64 modes, whole tiles)
   double* Hbuf = nullptr;  // one allocation holding all statics
   double* trbuf = nullptr;  // Gauss points: face traces, 4 faces x 5 fields x 5 ne
   double* U[2] = {nullptr, nullptr};

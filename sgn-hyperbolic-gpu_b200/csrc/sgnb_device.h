@@ -1,6 +1,7 @@
 // sgnb_device.h -- parameter blocks shared by the host code and the sm_100a kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace sgnb {
@@ -116,7 +117,63 @@ __device__ __forceinline__ void block_copy2(unsigned* d1, const unsigned* s1, un
   for (int r = 0; r < R2; ++r)
     if (tid + r * NT < W2) d2[tid + r * NT] = t2[r];
 }
+
+// Tile loads by the tensor-memory accelerator, completed on a shared-memory mbarrier
+// (one elected thread initialises it and issues the copies; every thread waits on its
+// phase with a bounded number of tries). Loads from this device's own buffers only, no
+// cluster multicast.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned mb) {
+  asm volatile("mbarrier.init.shared.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;\n" ::"r"(mb), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned mb, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(mb), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void mbar_inval(unsigned mb) {
+  asm volatile("mbarrier.inval.shared.b64 [%0];\n" ::"r"(mb) : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int x, int y,
+                                            int z, unsigned mb) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(mb)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y,
+                                            unsigned mb) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(mb)
+      : "memory");
+}
+// Tries before a tile-load wait gives up (each try waits a while in hardware): far more
+// than any load takes, so a give-up means a fault, reported as a non-finite result.
+constexpr int kTmaTries = 1 << 20;
 #endif
+
+// Tensor maps of a context's FP64 buffers for the fused kernels' tile loads on meshes that
+// are a whole number of 8x4 tiles: each state-sized buffer as [field][element row]
+// [Nx * 25 nodes] with an [5][4][200] box (one tile's 5 x 32 x 25 doubles, in the shared
+// layout), the nodal depth as [element row][Nx * 25] with a [4][200] box. ok = 0: none.
+struct TileMaps {
+  CUtensorMap U[2], K1[2], K2, K3, H;
+  int ok;
+};
 
 // Buffers of one fused launch.
 struct StageArgs {
@@ -260,10 +317,12 @@ cudaError_t launch_gauges_back(double* lam, const long long* nodes, int ng, cons
                                cudaStream_t s);
 
 // Launchers (one translation unit per arithmetic mode).
+// M: tensor maps of the buffers A names (the context's own), or nullptr (no tile loads
+// by the tensor-memory accelerator).
 cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A,
-                               cudaStream_t s);
+                               cudaStream_t s, const TileMaps* M = nullptr);
 cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A,
-                              cudaStream_t s);
+                              cudaStream_t s, const TileMaps* M = nullptr);
 cudaError_t prepare_fused_exact();
 cudaError_t prepare_fused_fast();
 cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A,

@@ -112,6 +112,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+
 // Read-only views of the stage inputs of one launch.
 struct StageIn {
   const double* __restrict__ in;
@@ -431,11 +432,17 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
 // FULL: the mesh is a whole number of tiles, so every tile is full and the per-item range
 // checks and their branches are compiled out (8 % off the end-point stage at 2048 x 1024).
+// TMA: the stage modes' own-node tiles (state, stage derivative, nodal depth) arrive by
+// tensor-memory-accelerator copies described by M (full tiles of the single-instance
+// kernel only).
 template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false,
-          bool GHOST = false, bool GAUSS = false, bool FULL = false>
+          bool GHOST = false, bool GAUSS = false, bool FULL = false, bool TMA = false>
 __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& A,
                                            int bx, int by, long long blk,
-                                           typename Tile<TX_, TY_, EXACT>::Smem& S) {
+                                           typename Tile<TX_, TY_, EXACT>::Smem& S,
+                                           const TileMaps* M = nullptr) {
+  static_assert(!TMA || (FULL && !GHOST && !GAUSS && MODE != MODE_RHS && TX_ == 8 && TY_ == 4),
+                "tile loads by the tensor-memory accelerator: full 8x4 tiles, stage modes");
   using T = Tile<TX_, TY_, EXACT>;
   constexpr int TX = T::TX, TY = T::TY, NHALO = T::NHALO, RUN = T::RUN;
   constexpr int NHIT = T::NHIT, NFACE = T::NFACE, NFIT = T::NFIT;
@@ -516,17 +523,38 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
   item_map();
 
   // ---- load phase --------------------------------------------------------------
+  // TMA: one thread issues the tile's three copies (stage: u and k; end point: k1 and k2;
+  // each [5][4][200] doubles, and the [4][200] nodal depths) on an mbarrier that aliases
+  // the (not yet used) reduction slots.
+  const unsigned mbar = smem_addr(&S.red[0][0]);
+  if constexpr (TMA) {
+    if (tid == 0) mbar_init(mbar);
+    __syncthreads();
+    if (tid == 0) {
+      const int x = ex0 * NPP;  // 16-byte aligned: 1600 bytes per tile column
+      mbar_expect_tx(mbar, (unsigned)((2 * NV + 1) * TE * NPP * sizeof(double)));
+      const CUtensorMap* mu = MODE == MODE_STAGE ? &M->U[cur] : &M->K1[cur];
+      const CUtensorMap* mg = MODE == MODE_STAGE ? (A.kin_k2 ? &M->K2 : &M->K1[cur]) : &M->K2;
+      tma_load_3d(smem_addr(&S.U[0][0][0]), mu, x, ey0, 0, mbar);
+      tma_load_3d(smem_addr(&S.G[0][0][0]), mg, x, ey0, 0, mbar);
+      tma_load_2d(smem_addr(&S.H[0][0]), &M->H, x, ey0, mbar);
+    }
+  }
   {
-    // Statics, and the state of the rhs and stage modes, arrive by asynchronous copies
-    // straight into shared memory: a tile's loads are all in flight at once without
-    // holding registers. The stage mode stages k in the (still unused) G area and forms
-    // u + (c dt) k in shared memory once the copies have landed.
+    // Otherwise the statics, and the state of the rhs and stage modes, arrive by
+    // per-thread asynchronous copies straight into shared memory: a tile's loads are all in
+    // flight at once without holding registers. The stage mode stages k in the (still
+    // unused) G area and forms u + (c dt) k in shared memory once the copies have landed.
+    if constexpr (!TMA) {
 #pragma unroll
-    for (int u = 0; u < NIT; ++u)
-      if (okk[u]) {
-        if (SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
-      }
-    if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) {
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          if (SGNB_INB(gof[u], Nd) && SGNB_INB(sof[u], TE * NPP)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+        }
+    }
+    if constexpr (TMA) {
+      // the tile copies above
+    } else if constexpr (MODE == MODE_RHS || MODE == MODE_STAGE) {
       const double* __restrict__ src = MODE == MODE_RHS ? I.in : I.u;
 #pragma unroll
       for (int v = 0; v < NV; ++v)
@@ -657,6 +685,22 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     for (int u = 0; u < NFIT; ++u)
       if (fq[u] >= 0 && SGNB_INB(fq[u], NFACE)) S.Hf[fq[u]] = fv[u];
     cp_async_wait_all();
+    if constexpr (TMA) {
+      bool landed = false;
+      for (int it = 0; it < kTmaTries && !landed; ++it) landed = mbar_try_wait(mbar, 0);
+      if (!landed) {
+        // the copies did not complete: this thread's items become NaN, so the launch's
+        // results are non-finite and the controller ends the run with that error
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+          for (int u = 0; u < NIT; ++u) {
+            (&S.U[v][0][0])[sof[u]] = nan;
+            (&S.G[v][0][0])[sof[u]] = nan;
+          }
+      }
+    }
     if constexpr (MODE == MODE_STAGE) {
       // u + (c dt) k for this thread's own items (rk.cpp:100-103), in shared memory
 #pragma unroll
@@ -705,6 +749,9 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
     }
   }
   __syncthreads();
+  if constexpr (TMA) {
+    if (tid == 0) mbar_inval(mbar);  // its slots serve the error reduction later
+  }
 
   const int i = lane;  // tile element of this lane
   const int ix = i % TX, iy = i / TX;
@@ -1011,6 +1058,18 @@ __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_raw);
   fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, FRIC, GHOST, GAUSS, FULL>(C, C, A, blockIdx.x, blockIdx.y,
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
+}
+
+// Stage modes on a mesh of whole tiles, with the own-node tiles loaded by the
+// tensor-memory accelerator from the context's buffers that M describes.
+template <int MODE, bool EXACT>
+__global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS)
+    k_fused_tma(const RhsConsts C, const StageArgs A, const __grid_constant__ TileMaps M) {
+  extern __shared__ __align__(128) unsigned char smem_tiles[];  // the copies' destinations
+  using T = Tile<8, 4, EXACT>;
+  typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_tiles);
+  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, false, false, false, true, true>(
+      C, C, A, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, S, &M);
 }
 
 // Face traces of every element for Gauss-Legendre points (sgn2d.cpp:141-177), of the

@@ -6,8 +6,9 @@
 
 namespace sgnb {
 namespace dev {
-cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
-  return launch_any(mode, C, A, s);
+cudaError_t launch_fused_exact(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s,
+                              const TileMaps* M) {
+  return launch_any(mode, C, A, s, M);
 }
 cudaError_t prepare_fused_exact() { return prepare_all(); }
 int fused_grid_blocks(int Nx, int Ny) { return ((Nx + 7) / 8) * ((Ny + 3) / 4); }

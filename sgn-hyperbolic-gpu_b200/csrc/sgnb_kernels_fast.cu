@@ -6,8 +6,9 @@
 
 namespace sgnb {
 namespace dev {
-cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
-  return launch_any(mode, C, A, s);
+cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s,
+                              const TileMaps* M) {
+  return launch_any(mode, C, A, s, M);
 }
 cudaError_t prepare_fused_fast() { return prepare_all(); }
 

@@ -9,7 +9,8 @@ namespace sgnb {
 namespace dev {
 
 template <int MODE>
-static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
+static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStream_t s,
+                               const TileMaps* M) {
   const dim3 grid((C.Nx + 7) / 8, (C.Ny + 3) / 4);
   const size_t smem = sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
   if (C.gauss) {
@@ -29,7 +30,16 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
       if (full) k_fused<MODE, SGNB_EXACT, false, true, false, true><<<grid, NTHR, smem, s>>>(C, A);
       else k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
     } else if (full) {
-      k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
+      // the stage modes' own-node tiles by the tensor-memory accelerator where the
+      // context's tensor maps describe the buffers
+      bool tma = false;
+      if constexpr (MODE != MODE_RHS) {
+        if (M != nullptr && M->ok) {
+          k_fused_tma<MODE, SGNB_EXACT><<<grid, NTHR, smem, s>>>(C, A, *M);
+          tma = true;
+        }
+      }
+      if (!tma) k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
     } else {
       k_fused<MODE, SGNB_EXACT, false, false><<<grid, NTHR, smem, s>>>(C, A);
     }
@@ -60,14 +70,24 @@ static cudaError_t prepare_all() {
   if (e == cudaSuccess) e = prepare_variant<true, false, true>();
   if (e == cudaSuccess) e = prepare_variant<false, false, false, true>();
   if (e == cudaSuccess) e = prepare_variant<false, true, false, true>();
+  {
+    const int bytes = (int)sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fused_tma<MODE_STAGE, SGNB_EXACT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fused_tma<MODE_FSAL, SGNB_EXACT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
   return e;
 }
 
-static cudaError_t launch_any(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s) {
+static cudaError_t launch_any(int mode, const RhsConsts& C, const StageArgs& A, cudaStream_t s,
+                              const TileMaps* M = nullptr) {
   switch (mode) {
-    case MODE_RHS: return launch_mode<MODE_RHS>(C, A, s);
-    case MODE_STAGE: return launch_mode<MODE_STAGE>(C, A, s);
-    case MODE_FSAL: return launch_mode<MODE_FSAL>(C, A, s);
+    case MODE_RHS: return launch_mode<MODE_RHS>(C, A, s, M);
+    case MODE_STAGE: return launch_mode<MODE_STAGE>(C, A, s, M);
+    case MODE_FSAL: return launch_mode<MODE_FSAL>(C, A, s, M);
     default: return cudaErrorInvalidValue;
   }
 }
