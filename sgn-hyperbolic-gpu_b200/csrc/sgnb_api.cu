@@ -11,6 +11,7 @@
 #include "sgnb_ctx.h"
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -49,6 +50,9 @@ struct Launch {
   int stage = 2;               // mode 1: 2 (k1 -> K2) or 3 (k2 -> K3)
 };
 
+static bool encode_state_map(const sgnb_ctx* c, CUtensorMap* m, const void* p,
+                             CUtensorMapDataType type, size_t elem, cuuint32_t nz);
+
 cudaError_t launch(sgnb_ctx* c, const Launch& L, cudaStream_t s) {
   if (c->mixed) {
     StageArgsM A{};
@@ -63,7 +67,7 @@ cudaError_t launch(sgnb_ctx* c, const Launch& L, cudaStream_t s) {
     A.coef = L.stage == 3 ? 0.75 : 0.5;
     if (L.mode == 0) A.out = L.out ? nullptr : A.K1[c->cur];  // no FP64 output: the FSAL head
     else A.out = L.stage == 3 ? A.K3 : A.K2;
-    return dev::launch_fused_mixed(L.mode, c->C, A, s);
+    return dev::launch_fused_mixed(L.mode, c->C, A, s, c->mapsM.ok ? &c->mapsM : nullptr);
   }
   StageArgs A{};
   A.U[0] = c->U[0]; A.U[1] = c->U[1];
@@ -75,7 +79,21 @@ cudaError_t launch(sgnb_ctx* c, const Launch& L, cudaStream_t s) {
   A.kin_k2 = L.stage == 3;
   A.coef = L.stage == 3 ? 0.75 : 0.5;
   A.out = L.mode == 0 ? L.out : (L.stage == 3 ? A.K3 : A.K2);
-  const TileMaps* M = c->maps.ok ? &c->maps : nullptr;  // A names the context's buffers
+  // tile copies by the tensor-memory accelerator: A names the context's buffers; the
+  // right-hand side's input gets its own map, encoded for this launch
+  const TileMaps* M = nullptr;
+  TileMaps Mr;
+  if (c->maps.ok) {
+    if (L.mode != 0) {
+      M = &c->maps;
+    } else if (L.in != nullptr) {
+      Mr = c->maps;
+      if (encode_state_map(c, &Mr.In, L.in, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, 5)) {
+        Mr.inOk = 1;
+        M = &Mr;
+      }
+    }
+  }
   return c->precision == SGNB_FP64_FAST ? dev::launch_fused_fast(L.mode, c->C, A, s, M)
                                         : dev::launch_fused_exact(L.mode, c->C, A, s, M);
 }
@@ -176,18 +194,38 @@ Mesh mesh_for(const sgnb_desc* d) {
   return m;
 }
 
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// A map of one state-sized buffer as [field][element row][Nx * 25] elements of `type` with
+// a [nz][4][200] box (nz = 5: one tile of every field; 1: one field).
+static bool encode_state_map(const sgnb_ctx* c, CUtensorMap* m, const void* p,
+                             CUtensorMapDataType type, size_t elem, cuuint32_t nz) {
+  const EncodeTiled enc = reinterpret_cast<EncodeTiled>(c->encode_tiled);
+  if (enc == nullptr || ((uintptr_t)p & 15) != 0) return false;
+  const cuuint64_t W = (cuuint64_t)c->desc.Nx * 25;
+  const cuuint64_t dim[3] = {W, (cuuint64_t)c->desc.Ny, 5};
+  const cuuint64_t stride[2] = {W * elem, (cuuint64_t)c->Nd * elem};
+  const cuuint32_t box[3] = {200, 4, nz};
+  const cuuint32_t one[3] = {1, 1, 1};
+  return enc(m, type, 3, const_cast<void*>(p), dim, stride, box, one,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Tensor maps of the context's buffers for the fused kernels' tile loads (meshes that are
 // a whole number of 8x4 tiles). The encoder comes from the driver through the runtime, so
 // the library links no driver library; without it (or on any encoding error), or with
 // SGNB_TMA=0 in the environment at creation, the kernels keep their per-thread
 // asynchronous copies (the same results bit for bit: data movement only).
 static void build_tile_maps(sgnb_ctx* c) {
-  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
   c->maps.ok = 0;
-  if (c->mixed || c->desc.Nx % 8 != 0 || c->desc.Ny % 4 != 0) return;
+  c->maps.inOk = 0;
+  c->mapsM.ok = 0;
+  c->encode_tiled = nullptr;
+  if (c->desc.Nx % 8 != 0 || c->desc.Ny % 4 != 0) return;
   const char* sw = std::getenv("SGNB_TMA");
   if (sw && sw[0] == '0') return;
   void* fn = nullptr;
@@ -198,29 +236,34 @@ static void build_tile_maps(sgnb_ctx* c) {
     cudaGetLastError();
     return;
   }
-  const Encode enc = reinterpret_cast<Encode>(fn);
-  const cuuint64_t W = (cuuint64_t)c->desc.Nx * 25, H = (cuuint64_t)c->desc.Ny;
-  // [field][element row][Nx * 25 doubles], box [5][4][200]: one 8x4 tile of every field
-  const cuuint64_t dim3[3] = {W, H, 5};
-  const cuuint64_t stride3[2] = {W * sizeof(double), (cuuint64_t)c->Nd * sizeof(double)};
-  const cuuint32_t box3[3] = {200, 4, 5};
-  const cuuint32_t one[3] = {1, 1, 1};
-  auto map3 = [&](CUtensorMap* m, const void* p) {
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(p), dim3, stride3, box3,
-               one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+  c->encode_tiled = fn;
+  const EncodeTiled enc = reinterpret_cast<EncodeTiled>(fn);
+  // the nodal depth: [element row][Nx * 25] doubles, box [4][200]
+  const cuuint64_t dim2[2] = {(cuuint64_t)c->desc.Nx * 25, (cuuint64_t)c->desc.Ny};
+  const cuuint64_t stride2[1] = {dim2[0] * sizeof(double)};
+  const cuuint32_t box2[2] = {200, 4};
+  const cuuint32_t one[2] = {1, 1};
+  auto mapH = [&](CUtensorMap* m) {
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(c->C.Hnod), dim2,
+               stride2, box2, one, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
            CUDA_SUCCESS;
   };
-  const cuuint64_t dim2[2] = {W, H};
-  const cuuint64_t stride2[1] = {W * sizeof(double)};
-  const cuuint32_t box2[2] = {200, 4};
-  bool ok = map3(&c->maps.U[0], c->U[0]) && map3(&c->maps.U[1], c->U[1]) &&
-            map3(&c->maps.K1[0], c->K1[0]) && map3(&c->maps.K1[1], c->K1[1]) &&
-            map3(&c->maps.K2, c->K2) && map3(&c->maps.K3, c->K3);
-  ok = ok && enc(&c->maps.H, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(c->C.Hnod),
-                 dim2, stride2, box2, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  const auto F64 = CU_TENSOR_MAP_DATA_TYPE_FLOAT64, F32 = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  if (c->mixed) {
+    const bool okm = encode_state_map(c, &c->mapsM.K1[0], c->K1[0], F32, 4, 1) &&
+                     encode_state_map(c, &c->mapsM.K1[1], c->K1[1], F32, 4, 1) &&
+                     encode_state_map(c, &c->mapsM.K2, c->K2, F32, 4, 1) &&
+                     encode_state_map(c, &c->mapsM.K3, c->K3, F32, 4, 1) && mapH(&c->mapsM.H);
+    c->mapsM.ok = okm ? 1 : 0;
+    return;
+  }
+  const bool ok = encode_state_map(c, &c->maps.U[0], c->U[0], F64, 8, 5) &&
+                  encode_state_map(c, &c->maps.U[1], c->U[1], F64, 8, 5) &&
+                  encode_state_map(c, &c->maps.K1[0], c->K1[0], F64, 8, 5) &&
+                  encode_state_map(c, &c->maps.K1[1], c->K1[1], F64, 8, 5) &&
+                  encode_state_map(c, &c->maps.K2, c->K2, F64, 8, 5) &&
+                  encode_state_map(c, &c->maps.K3, c->K3, F64, 8, 5) && mapH(&c->maps.H);
   c->maps.ok = ok ? 1 : 0;
 }
 

@@ -21,6 +21,8 @@ struct sgnb_ctx {
   long long Nd = 0, ntot = 0;
   sgnb::RhsConsts C{};
   sgnb::TileMaps maps{};  // tensor maps of U, K1, K2, K3, Hnod (FP64 modes, whole tiles)
+  sgnb::TileMapsM mapsM{};  // the mixed mode's (FP32 K1, K2, K3; Hnod)
+  void* encode_tiled = nullptr;  // the driver's tensor-map encoder (set with the maps)
   double* Hbuf = nullptr;  // one allocation holding all statics
   double* trbuf = nullptr;  // Gauss points: face traces, 4 faces x 5 fields x 5 ne
   double* U[2] = {nullptr, nullptr};

@@ -170,8 +170,18 @@ constexpr int kTmaTries = 1 << 20;
 // are a whole number of 8x4 tiles: each state-sized buffer as [field][element row]
 // [Nx * 25 nodes] with an [5][4][200] box (one tile's 5 x 32 x 25 doubles, in the shared
 // layout), the nodal depth as [element row][Nx * 25] with a [4][200] box. ok = 0: none.
+// In: the right-hand-side mode's input (any 16-byte-aligned device state, encoded per
+// launch); inOk = 0: none.
 struct TileMaps {
-  CUtensorMap U[2], K1[2], K2, K3, H;
+  CUtensorMap U[2], K1[2], K2, K3, H, In;
+  int ok, inOk;
+};
+
+// The mixed-precision mode's counterparts (intermediate stage): the FP32 stage buffers as
+// [field][element row][Nx * 25] with a [1][4][200] box (one field of one tile per copy),
+// the nodal depth as for the FP64 kernels.
+struct TileMapsM {
+  CUtensorMap K1[2], K2, K3, H;
   int ok;
 };
 
@@ -326,7 +336,7 @@ cudaError_t launch_fused_fast(int mode, const RhsConsts& C, const StageArgs& A,
 cudaError_t prepare_fused_exact();
 cudaError_t prepare_fused_fast();
 cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A,
-                               cudaStream_t s);
+                               cudaStream_t s, const TileMapsM* M = nullptr);
 cudaError_t prepare_fused_mixed();
 int fused_grid_blocks(int Nx, int Ny);
 // Batched launch (FP64 fast): tile shape shape_id (0: 8x4, 1: 16x2, 2: 4x8); `blocks`

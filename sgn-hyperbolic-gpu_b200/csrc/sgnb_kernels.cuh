@@ -432,7 +432,7 @@ __device__ __forceinline__ void mirror(const double* own, double* ghost) {
 // batched kernel. Returns early (uniformly over the CTA) when the instance's run is done.
 // FULL: the mesh is a whole number of tiles, so every tile is full and the per-item range
 // checks and their branches are compiled out (8 % off the end-point stage at 2048 x 1024).
-// TMA: the stage modes' own-node tiles (state, stage derivative, nodal depth) arrive by
+// TMA: the own-node tiles (state or stage derivatives, nodal depth) arrive by
 // tensor-memory-accelerator copies described by M (full tiles of the single-instance
 // kernel only).
 template <int MODE, bool EXACT, int TX_, int TY_, class TC, class TB, class TA, bool FRIC = false,
@@ -441,8 +441,8 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_, EXACT>::Smem& S,
                                            const TileMaps* M = nullptr) {
-  static_assert(!TMA || (FULL && !GHOST && !GAUSS && MODE != MODE_RHS && TX_ == 8 && TY_ == 4),
-                "tile loads by the tensor-memory accelerator: full 8x4 tiles, stage modes");
+  static_assert(!TMA || (FULL && !GHOST && !GAUSS && TX_ == 8 && TY_ == 4),
+                "tile loads by the tensor-memory accelerator: full 8x4 tiles");
   using T = Tile<TX_, TY_, EXACT>;
   constexpr int TX = T::TX, TY = T::TY, NHALO = T::NHALO, RUN = T::RUN;
   constexpr int NHIT = T::NHIT, NFACE = T::NFACE, NFIT = T::NFIT;
@@ -523,20 +523,23 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
   item_map();
 
   // ---- load phase --------------------------------------------------------------
-  // TMA: one thread issues the tile's three copies (stage: u and k; end point: k1 and k2;
-  // each [5][4][200] doubles, and the [4][200] nodal depths) on an mbarrier that aliases
-  // the (not yet used) reduction slots.
+  // TMA: one thread issues the tile's copies (rhs: the input; stage: u and k; end point: k1
+  // and k2; each [5][4][200] doubles; and the [4][200] nodal depths) on an mbarrier that
+  // aliases the (not yet used) reduction slots.
   const unsigned mbar = smem_addr(&S.red[0][0]);
   if constexpr (TMA) {
     if (tid == 0) mbar_init(mbar);
     __syncthreads();
     if (tid == 0) {
       const int x = ex0 * NPP;  // 16-byte aligned: 1600 bytes per tile column
-      mbar_expect_tx(mbar, (unsigned)((2 * NV + 1) * TE * NPP * sizeof(double)));
-      const CUtensorMap* mu = MODE == MODE_STAGE ? &M->U[cur] : &M->K1[cur];
-      const CUtensorMap* mg = MODE == MODE_STAGE ? (A.kin_k2 ? &M->K2 : &M->K1[cur]) : &M->K2;
+      constexpr int narr = MODE == MODE_RHS ? 1 : 2;
+      mbar_expect_tx(mbar, (unsigned)((narr * NV + 1) * TE * NPP * sizeof(double)));
+      const CUtensorMap* mu = MODE == MODE_RHS ? &M->In : (MODE == MODE_STAGE ? &M->U[cur] : &M->K1[cur]);
       tma_load_3d(smem_addr(&S.U[0][0][0]), mu, x, ey0, 0, mbar);
-      tma_load_3d(smem_addr(&S.G[0][0][0]), mg, x, ey0, 0, mbar);
+      if constexpr (MODE != MODE_RHS) {
+        const CUtensorMap* mg = MODE == MODE_STAGE ? (A.kin_k2 ? &M->K2 : &M->K1[cur]) : &M->K2;
+        tma_load_3d(smem_addr(&S.G[0][0][0]), mg, x, ey0, 0, mbar);
+      }
       tma_load_2d(smem_addr(&S.H[0][0]), &M->H, x, ey0, mbar);
     }
   }

@@ -30,16 +30,12 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
       if (full) k_fused<MODE, SGNB_EXACT, false, true, false, true><<<grid, NTHR, smem, s>>>(C, A);
       else k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
     } else if (full) {
-      // the stage modes' own-node tiles by the tensor-memory accelerator where the
-      // context's tensor maps describe the buffers
-      bool tma = false;
-      if constexpr (MODE != MODE_RHS) {
-        if (M != nullptr && M->ok) {
-          k_fused_tma<MODE, SGNB_EXACT><<<grid, NTHR, smem, s>>>(C, A, *M);
-          tma = true;
-        }
-      }
-      if (!tma) k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
+      // the own-node tiles by the tensor-memory accelerator where the context's tensor
+      // maps describe the buffers (and, for the rhs mode, a map of its input)
+      if (M != nullptr && M->ok && (MODE != MODE_RHS || M->inOk))
+        k_fused_tma<MODE, SGNB_EXACT><<<grid, NTHR, smem, s>>>(C, A, *M);
+      else
+        k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
     } else {
       k_fused<MODE, SGNB_EXACT, false, false><<<grid, NTHR, smem, s>>>(C, A);
     }
@@ -72,6 +68,9 @@ static cudaError_t prepare_all() {
   if (e == cudaSuccess) e = prepare_variant<false, true, false, true>();
   {
     const int bytes = (int)sizeof(Tile<8, 4, SGNB_EXACT>::Smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fused_tma<MODE_RHS, SGNB_EXACT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_fused_tma<MODE_STAGE, SGNB_EXACT>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

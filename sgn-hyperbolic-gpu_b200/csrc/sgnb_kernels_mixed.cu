@@ -6,12 +6,25 @@ namespace sgnb {
 namespace dev {
 
 template <int MODE>
-static cudaError_t launch_m(const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
+static cudaError_t launch_m(const RhsConsts& C, const StageArgsM& A, cudaStream_t s,
+                            const TileMapsM* M) {
   const dim3 grid((C.Nx + mix::TX - 1) / mix::TX, (C.Ny + mix::TY - 1) / mix::TY);
-  if (C.manning) mix::k_mixed<MODE, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
-  else if (C.Nx % mix::TX == 0 && C.Ny % mix::TY == 0)  // every tile full
-    mix::k_mixed<MODE, false, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
-  else mix::k_mixed<MODE, false><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  if (C.manning) {
+    mix::k_mixed<MODE, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  } else if (C.Nx % mix::TX == 0 && C.Ny % mix::TY == 0) {  // every tile full
+    bool tma = false;
+    // the intermediate stage's tiles by the tensor-memory accelerator (the end-point stage
+    // was 1.4 % slower so: its per-thread copies land in five scattered areas)
+    if constexpr (MODE == mix::MODE_STAGE) {
+      if (M != nullptr && M->ok) {
+        mix::k_mixed_tma<MODE><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A, *M);
+        tma = true;
+      }
+    }
+    if (!tma) mix::k_mixed<MODE, false, true><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  } else {
+    mix::k_mixed<MODE, false><<<grid, mix::NTHR, sizeof(mix::Smem), s>>>(C, A);
+  }
   return cudaGetLastError();
 }
 
@@ -32,11 +45,12 @@ cudaError_t read_oob_mixed(unsigned long long* out, bool reset) {
 #endif
 }
 
-cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A, cudaStream_t s) {
+cudaError_t launch_fused_mixed(int mode, const RhsConsts& C, const StageArgsM& A, cudaStream_t s,
+                               const TileMapsM* M) {
   switch (mode) {
-    case 0: return launch_m<mix::MODE_RHS>(C, A, s);
-    case 1: return launch_m<mix::MODE_STAGE>(C, A, s);
-    case 2: return launch_m<mix::MODE_FSAL>(C, A, s);
+    case 0: return launch_m<mix::MODE_RHS>(C, A, s, M);
+    case 1: return launch_m<mix::MODE_STAGE>(C, A, s, M);
+    case 2: return launch_m<mix::MODE_FSAL>(C, A, s, M);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -58,6 +72,9 @@ static cudaError_t prepare_mixed_fric() {
 cudaError_t prepare_fused_mixed() {
   cudaError_t e = prepare_mixed_fric<false>();
   if (e == cudaSuccess) e = prepare_mixed_fric<false, true>();
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(mix::k_mixed_tma<mix::MODE_STAGE>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mix::Smem));
   return e == cudaSuccess ? prepare_mixed_fric<true>() : e;
 }
 

@@ -285,9 +285,15 @@ __device__ __forceinline__ void line_mixed(const TC& C, const TB& Tb, const doub
 // One tile (bx, by) of the mixed-precision right-hand side / stage kernel, error partial
 // slot blk. Shared by the single-instance kernel and the batched kernel. FULL: the mesh is
 // a whole number of tiles (the per-item range checks are compiled out).
-template <int MODE, class TC, class TB, class TA, bool FRIC = false, bool FULL = false>
+// TMA: the intermediate stage's nodal depths and FP32 stage derivatives arrive by
+// tensor-memory-accelerator copies described by M (full tiles of the single-instance
+// kernel only).
+template <int MODE, class TC, class TB, class TA, bool FRIC = false, bool FULL = false,
+          bool TMA = false>
 __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& A, int bx, int by,
-                                           long long blk, Smem& S) {
+                                           long long blk, Smem& S,
+                                           const TileMapsM* M = nullptr) {
+  static_assert(!TMA || (FULL && MODE == MODE_STAGE), "tile copies: full tiles, intermediate stage");
 
   int cur = 0;
   double atol = 0.0, rtol = 0.0;
@@ -352,13 +358,29 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
   item_map();
 
   // ---- load phase ----------------------------------------------------------------
+  const unsigned mbar = smem_addr(&S.red[0][0]);  // TMA: the tile copies' barrier
   {
-    // statics by asynchronous copies straight into shared memory
-#pragma unroll
-    for (int u = 0; u < NIT; ++u)
-      if (okk[u]) {
-        if (SGNB_INB(gof[u], Nd)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+    // statics by asynchronous copies straight into shared memory (TMA: one thread copies
+    // the nodal depths and the stage derivative, one field of the tile per copy, on an
+    // mbarrier that aliases the not yet used reduction slots)
+    if constexpr (TMA) {
+      if (tid == 0) mbar_init(mbar);
+      __syncthreads();
+      if (tid == 0) {
+        const int x = ex0 * NPP;  // 16-byte aligned: 800 bytes of FP32 per tile column
+        mbar_expect_tx(mbar, (unsigned)(TE * NPP * (sizeof(double) + NV * sizeof(float))));
+        tma_load_2d(smem_addr(&S.H[0][0]), &M->H, x, ey0, mbar);
+        const CUtensorMap* mk = A.kin_k2 ? &M->K2 : &M->K1[cur];
+#pragma unroll 1
+        for (int v = 0; v < NV; ++v) tma_load_3d(smem_addr(&S.G[v][0][0]), mk, x, ey0, v, mbar);
       }
+    } else {
+#pragma unroll
+      for (int u = 0; u < NIT; ++u)
+        if (okk[u]) {
+          if (SGNB_INB(gof[u], Nd)) cp_async8(&(&S.H[0][0])[sof[u]], C.Hnod + gof[u]);
+        }
+    }
     // halos: the neighbour tiles' trace nodes, stage inputs formed in registers
     double hv[NHIT];
     int hq[NHIT];
@@ -481,7 +503,7 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
       }
     }
     double* __restrict__ unew = A.U[cur ^ 1];
-    if constexpr (MODE == MODE_STAGE) {
+    if constexpr (MODE == MODE_STAGE && !TMA) {
       // k (FP32) by asynchronous copies into the still unused G area
 #pragma unroll
       for (int v = 0; v < NV; ++v)
@@ -533,6 +555,19 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
             if constexpr (MODE == MODE_FSAL) k3x[v][u] = (I.k3 + (long long)v * Nd)[gof[u]];
           }
       cp_async_wait_all();  // k (k1, k2) and the statics have landed
+      if constexpr (TMA) {
+        bool landed = false;
+        for (int it = 0; it < kTmaTries && !landed; ++it) landed = mbar_try_wait(mbar, 0);
+        if (!landed) {
+          // the copies did not complete: this thread's state items become NaN, so the
+          // launch's results are non-finite and the controller ends the run with that error
+          const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+          for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int u = 0; u < NIT; ++u) ux[v][u] = nan;
+        }
+      }
     }
     // fields in the order 3, 4, 0, 1, 2: the end-point stage's field-4 derivatives sit in
     // the d area, which fields 1 and 2 overwrite after the barrier
@@ -582,6 +617,9 @@ __device__ __forceinline__ void mixed_tile(const TC& C, const TB& Tb, const TA& 
     cp_async_wait_all();
   }
   __syncthreads();
+  if constexpr (TMA) {
+    if (tid == 0) mbar_inval(mbar);  // its slots serve the error reduction later
+  }
 
   const int i = lane;
   const int ix = i % TX, iy = i / TX;
@@ -834,6 +872,18 @@ __global__ void __launch_bounds__(NTHR, SGNB_MIXED_MIN_CTAS) k_mixed(const RhsCo
   Smem& S = *reinterpret_cast<Smem*>(smem_raw);
   mixed_tile<MODE, RhsConsts, RhsConsts, StageArgsM, FRIC, FULL>(
       C, C, A, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
+}
+
+// Intermediate stage on a mesh of whole tiles, with the nodal depths and the stage
+// derivative loaded by the tensor-memory accelerator from the context's buffers that M
+// describes.
+template <int MODE>
+__global__ void __launch_bounds__(NTHR, SGNB_MIXED_MIN_CTAS)
+    k_mixed_tma(const RhsConsts C, const StageArgsM A, const __grid_constant__ TileMapsM M) {
+  extern __shared__ __align__(128) unsigned char smem_tiles_m[];  // the copies' destinations
+  Smem& S = *reinterpret_cast<Smem*>(smem_tiles_m);
+  mixed_tile<MODE, RhsConsts, RhsConsts, StageArgsM, false, true, true>(
+      C, C, A, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, S, &M);
 }
 
 // Batched form (8x4 tiles): the work list of BatchArgsM, per tile the instance's constants

@@ -44,3 +44,29 @@ def test_tile_copies_bitwise(prec, bc):
     assert sa == sb and sa[0] == 8
     assert np.isfinite(a).all()
     assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def rhs_pair(prec, kw, U, tma):
+    old = os.environ.get("SGNB_TMA")
+    os.environ["SGNB_TMA"] = "1" if tma else "0"
+    try:
+        with sgnb.SGN2DB200(precision=prec, **kw) as d:
+            d.upload(U)
+            a = d.rhs_once()  # input: the context's state buffer
+            b = d.rhs(U)      # input: the context's scratch (host round trip)
+            return a, b
+    finally:
+        if old is None:
+            del os.environ["SGNB_TMA"]
+        else:
+            os.environ["SGNB_TMA"] = old
+
+
+@pytest.mark.parametrize("prec", [sgnb.FP64_EXACT, sgnb.FP64_FAST])
+def test_rhs_tile_copies_bitwise(prec):
+    """The right-hand-side mode with its input's map encoded per launch."""
+    kw, U = bump_case(1, Nx=24, Ny=16, Lx=12.0, Ly=8.0)
+    a1, b1 = rhs_pair(prec, kw, U, True)
+    a0, b0 = rhs_pair(prec, kw, U, False)
+    for x, y in ((a1, a0), (b1, b0), (a1, b1)):
+        assert np.array_equal(np.asarray(x).view(np.uint64), np.asarray(y).view(np.uint64))
