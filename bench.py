@@ -245,7 +245,7 @@ def run_ours(args):
     achieved = bpd[dominant] * dof / per[dominant] / 1e9
     tpd = traffic_per_dof()
     traffic = tpd.get(dominant) if args.precision != "mixed" else None
-    roofline = {"bound": "hbm", "kernel": f"k_fused ({dominant} mode)",
+    roofline = {"bound": "hbm", "kernel": f"k_fused_tma ({dominant} mode; k_fused on meshes of partial tiles)",
                 "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": (round(traffic * dof) if traffic else None),
