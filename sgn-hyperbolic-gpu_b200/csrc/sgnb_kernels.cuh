@@ -441,7 +441,7 @@ __device__ __forceinline__ void fused_tile(const TC& C, const TB& Tb, const TA& 
                                            int bx, int by, long long blk,
                                            typename Tile<TX_, TY_, EXACT>::Smem& S,
                                            const TileMaps* M = nullptr) {
-  static_assert(!TMA || (FULL && !GHOST && !GAUSS && TX_ == 8 && TY_ == 4),
+  static_assert(!TMA || (FULL && !GAUSS && TX_ == 8 && TY_ == 4),
                 "tile loads by the tensor-memory accelerator: full 8x4 tiles");
   using T = Tile<TX_, TY_, EXACT>;
   constexpr int TX = T::TX, TY = T::TY, NHALO = T::NHALO, RUN = T::RUN;
@@ -1063,15 +1063,15 @@ __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS) k_fused(
                                 (long long)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
-// Stage modes on a mesh of whole tiles, with the own-node tiles loaded by the
-// tensor-memory accelerator from the context's buffers that M describes.
-template <int MODE, bool EXACT>
+// A mesh of whole tiles, with the own-node tiles loaded by the tensor-memory accelerator
+// from the buffers that M describes. GHOST: slab edges compiled in (x-slab contexts).
+template <int MODE, bool EXACT, bool GHOST = false>
 __global__ void __launch_bounds__(NTHR, EXACT ? 2 : SGNB_FAST_MIN_CTAS)
     k_fused_tma(const RhsConsts C, const StageArgs A, const __grid_constant__ TileMaps M) {
   extern __shared__ __align__(128) unsigned char smem_tiles[];  // the copies' destinations
   using T = Tile<8, 4, EXACT>;
   typename T::Smem& S = *reinterpret_cast<typename T::Smem*>(smem_tiles);
-  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, false, false, false, true, true>(
+  fused_tile<MODE, EXACT, 8, 4, RhsConsts, RhsConsts, StageArgs, false, GHOST, false, true, true>(
       C, C, A, blockIdx.x, blockIdx.y, (long long)blockIdx.y * gridDim.x + blockIdx.x, S, &M);
 }
 

@@ -26,13 +26,15 @@ static cudaError_t launch_mode(const RhsConsts& C, const StageArgs& A, cudaStrea
     else k_fused<MODE, SGNB_EXACT, true, false><<<grid, NTHR, smem, s>>>(C, A);
   } else {
     const bool full = C.Nx % 8 == 0 && C.Ny % 4 == 0;  // every tile full
+    // the own-node tiles by the tensor-memory accelerator where the context's tensor maps
+    // describe the buffers (and, for the rhs mode, a map of its input)
+    const bool tma = full && M != nullptr && M->ok && (MODE != MODE_RHS || M->inOk);
     if (ghost) {
-      if (full) k_fused<MODE, SGNB_EXACT, false, true, false, true><<<grid, NTHR, smem, s>>>(C, A);
+      if (tma) k_fused_tma<MODE, SGNB_EXACT, true><<<grid, NTHR, smem, s>>>(C, A, *M);
+      else if (full) k_fused<MODE, SGNB_EXACT, false, true, false, true><<<grid, NTHR, smem, s>>>(C, A);
       else k_fused<MODE, SGNB_EXACT, false, true><<<grid, NTHR, smem, s>>>(C, A);
     } else if (full) {
-      // the own-node tiles by the tensor-memory accelerator where the context's tensor
-      // maps describe the buffers (and, for the rhs mode, a map of its input)
-      if (M != nullptr && M->ok && (MODE != MODE_RHS || M->inOk))
+      if (tma)
         k_fused_tma<MODE, SGNB_EXACT><<<grid, NTHR, smem, s>>>(C, A, *M);
       else
         k_fused<MODE, SGNB_EXACT, false, false, false, true><<<grid, NTHR, smem, s>>>(C, A);
@@ -76,6 +78,15 @@ static cudaError_t prepare_all() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(k_fused_tma<MODE_FSAL, SGNB_EXACT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fused_tma<MODE_RHS, SGNB_EXACT, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fused_tma<MODE_STAGE, SGNB_EXACT, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fused_tma<MODE_FSAL, SGNB_EXACT, true>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   }
   return e;
