@@ -120,8 +120,8 @@ __device__ __forceinline__ void block_copy2(unsigned* d1, const unsigned* s1, un
 
 // Tile loads by the tensor-memory accelerator, completed on a shared-memory mbarrier
 // (one elected thread initialises it and issues the copies; every thread waits on its
-// phase with a bounded number of tries). Loads from this device's own buffers only, no
-// cluster multicast.
+// phase with a bounded number of tries). Loads from this device's own buffers only, each
+// into the issuing CTA's own shared memory.
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
